@@ -1,0 +1,268 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 circulant-embedding path.
+
+Workload (one step = one realization): 3D Matern nu=1.5 (`matern32`), sigma^2=1,
+axiparallel correlation lengths (0.2, 0.1, 0.05) on [0,1]^3 with 256^3 cells,
+embedding factor 2 (512^3 torus).  FP64 spectrum (built once, untimed), FP32
+realizations with seeded on-device noise.  Metric: field cells/s.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+--impl reference times the FP64 CPU restatement of the reference's algorithm
+(oracle/) on the host cores (the reference itself needs FFTW-MPI, MPI and
+dune-common, which this image lacks).  Under torchrun each rank runs an
+independent replica (no data-path collective); rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "parafields-core_b200"))
+
+WORKLOAD = dict(dim=3, cells=(256, 256, 256), covariance="matern32", variance=1.0,
+                corr_length=(0.2, 0.1, 0.05), anisotropy="axiparallel", embedding_factor=2)
+METRIC = "field cells/s (3D Matern-3/2 256^3 realization, 512^3 torus)"
+CONFIG = {"workload": "3d-matern32-axiparallel-256^3-factor2-fp32-realizations",
+          "cells": [256, 256, 256], "torus": [512, 512, 512], "spectrum": "fp64 DCT-I (untimed, once)",
+          "noise": "counter-based Philox2x32-10 on device, seed per step",
+          "l2": "no flush: per-step traffic ~1 GB through intermediates of 269 MB and 135 MB (> 126 MB L2)"}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """per-launch DRAM bytes of each kernel from the committed ncu summary, if any"""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    out = {}
+    if os.path.exists(p):
+        for line in open(p):
+            parts = line.split()
+            if len(parts) == 2 and not line.startswith("#"):
+                out[parts[0]] = float(parts[1])
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (clocks + throttle reasons)."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = f"/tmp/pf_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines()]
+            sm = [float(r[0]) for r in rows]
+            mx = float(rows[0][1])
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[3 + i]})
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons, "samples": len(sm)}
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+
+
+def dist_setup(n):
+    import torch
+    import torch.distributed as dist
+    if n > 1 or "WORLD_SIZE" in os.environ:
+        rank = int(os.environ.get("RANK", 0))
+        local = int(os.environ.get("LOCAL_RANK", 0))
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        return rank, dist.get_world_size(), local
+    return 0, 1, 0
+
+
+def cpu_oracle_realization(threads):
+    """one FP64 realization of the workload with the CPU restatement (spectrum untimed)"""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import pfb200
+    O.set_threads(threads)
+    d = pfb200.make_desc(**WORKLOAD)
+    g = O.resolve(d)
+    lam, _, _ = O.spectrum(d)
+    noise = O.noise(1, g.noise)
+    t0 = time.perf_counter()
+    O.generate(d, lam, noise)
+    return time.perf_counter() - t0, g.domain
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import pfb200
+    O.set_threads(threads)
+    d = pfb200.make_desc(**WORKLOAD)
+    g = O.resolve(d)
+    lam, _, _ = O.spectrum(d)
+    noise = O.noise(1, g.noise)
+    for _ in range(args.warmup):
+        O.generate(d, lam, noise)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.generate(d, lam, noise)
+    dt = time.perf_counter() - t0
+    v = g.domain * args.steps / dt
+    line = {"metric": METRIC, "value": v, "unit": "cells/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": CONFIG,
+            "cpu_baseline": {"value": v, "unit": "cells/s", "cores": threads, "kind": "port",
+                             "sample": "each step = 1 full FP64 realization (c2r of the 257x512x512 half "
+                                       "spectrum + extraction); noise drawn outside the timed region"},
+            "e2e": {"value": v, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "FP64 CPU restatement of the reference algorithm (FFTW-MPI/MPI/dune-common are not "
+                    "installed, so the reference itself cannot be built)"}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+    import pfb200
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    d = pfb200.make_desc(**WORKLOAD, precision=pfb200.PREC_F32)
+    P = pfb200.Plan(d)
+    P.set_stream(stream.cuda_stream)
+    P.spectrum_build()
+    n = P.info.domain_size
+    out = torch.empty(n, dtype=torch.float32, device=dev)
+    seed0 = 1000003 * (rank + 1)
+    for i in range(args.warmup):
+        P.generate(seed=seed0 + i, out=out)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    P.profile(True)
+    l0 = P.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i in range(args.steps):
+            P.generate(seed=seed0 + 100 + i, out=out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = P.launch_count() - l0
+    prof = P.profile_read()
+    P.profile(False)
+    t = torch.tensor([ms], device=dev)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms = float(t.item())
+    value = world * n * args.steps / (ms / 1e3)
+
+    # end to end through the public call with a host result buffer (D2H inside the region)
+    host = np.empty(n, dtype=np.float32)
+    host_pinned = torch.empty(n, dtype=torch.float32).pin_memory()
+    hp = host_pinned.numpy()
+    P.generate(seed=7, out=hp)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ke = max(2, min(args.steps, 10))
+    for i in range(ke):
+        P.generate(seed=seed0 + 500 + i, out=hp)
+    dt = time.perf_counter() - t0
+    te = torch.tensor([dt], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e = world * n * ke / float(te.item())
+    del host
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        dom = max(prof, key=lambda r: r["total_ms"]) if prof else None
+        roof = None
+        if dom:
+            avg_ms = dom["total_ms"] / dom["launches"]
+            bytes_per = dom["bytes"] / dom["launches"]
+            ach = bytes_per / (avg_ms / 1e3) / 1e9
+            tr = ncu_traffic().get(dom["name"])
+            roof = {"kernel": dom["name"], "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
+                    "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach / peak, 4),
+                    "traffic": tr, "algorithmic_bytes_per_launch": bytes_per, "avg_launch_ms": avg_ms,
+                    "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()}
+                                for r in prof]}
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            threads = os.cpu_count() or 1
+            dt_cpu, cells = cpu_oracle_realization(threads)
+            cpu = {"value": cells / dt_cpu, "unit": "cells/s", "cores": threads, "kind": "port",
+                   "sample": "1 FP64 realization of the same workload by the CPU restatement (oracle/), "
+                             f"{dt_cpu:.1f} s; spectrum and noise drawn outside the timed region"}
+        clocks = clk.summary()
+        line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": dict(CONFIG, parallelism=f"replicas{world}"),
+                "e2e": {"value": e2e, "unit": "cells/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": n * 4,
+                        "note": "pf_generate(seed, host out): seed passed by value, field copied to host"},
+                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+                "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"],
+                           "reasons": clocks["reasons"]}}
+        print(json.dumps(line), flush=True)
+    P.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,283 @@
+/*
+ * parafields_b200.h -- C ABI of the single-GPU (B200, sm_100a) circulant-embedding
+ * path of parafields-core.
+ *
+ * The reference exposes this path as the C++ template class
+ *   parafields::Matrix<Traits, MatrixBackend, FieldBackend>   (include/parafields/matrix.hh:55-133)
+ * plugged into RandomField<GridTraits, IsoMatrix, AnisoMatrix> (include/parafields/randomfield.hh:42-47).
+ * Its per-element backend concept (set/eval/mult called inside host loops,
+ * matrix.hh:378-404) cannot be honoured by a GPU, so the drop-in sits at the Matrix level:
+ * every entry point below replaces one Matrix member (cited per function), and the
+ * C++ facade in parafields-core_b200/include/parafields_b200/ maps the reference's
+ * Dune::ParameterTree keys and RandomField methods onto these calls.
+ *
+ * Conventions (all identical to the reference, single MPI rank):
+ *  - multi-dimensional arrays are stored with dimension 0 fastest
+ *    (fieldtraits.hh:400-430, indicesToIndex / indexToIndices);
+ *  - extended (torus) cells T_i = embedding_factor * cells_i (fieldtraits.hh:269-272);
+ *  - every forward transform divides by N = prod T_i, backward transforms are
+ *    unnormalised (r2cmatrixbackend.hh:279-282, r2cfieldbackend.hh:233-236), so
+ *    pf_matvec(PF_OP_MUL) returns (C_ext x)/N restricted to the domain, exactly as
+ *    Matrix::operator* does (matrix.hh:142-151, 1443-1501);
+ *  - spectra and noise use the reference's storage order, including the 3D
+ *    "transposed" frequency layout (fftw.transposed, fieldtraits.hh:229-267).
+ *
+ * Errors: every function returns a pf_status; pf_last_error_string() gives the
+ * message of the last failure on the calling thread.  PF_ERR_NEG_EIGEN carries the
+ * text of the reference's NegativeEigenvalueError (matrix.hh:307-315).
+ *
+ * Threading: one plan is used by one host thread at a time (the reference's Matrix
+ * is not thread-safe either, matrix.hh:87-90); distinct plans are independent.
+ */
+#ifndef PARAFIELDS_B200_H
+#define PARAFIELDS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pf_status {
+  PF_OK = 0,
+  PF_ERR_NEG_EIGEN = 1,     /* NegativeEigenvalueError, exceptions.hh:8-15 */
+  PF_ERR_CONFIG = 2,        /* std::runtime_error for an invalid configuration */
+  PF_ERR_OOM = 3,           /* device or pinned-host allocation failed */
+  PF_ERR_CUDA = 4,          /* a CUDA runtime call failed */
+  PF_ERR_NOT_CONVERGED = 5, /* CG hit its iteration cap without the requested residual */
+  PF_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up */
+  PF_ERR_STATE = 7,         /* call order violated (e.g. spectrum missing) */
+  PF_ERR_ARG = 8            /* null pointer / size mismatch */
+} pf_status;
+
+/* stochastic.covariance (matrix.hh:232-260) */
+typedef enum pf_covariance {
+  PF_COV_EXPONENTIAL = 0,
+  PF_COV_GAUSSIAN = 1,
+  PF_COV_SPHERICAL = 2,
+  PF_COV_SEPARABLE_EXPONENTIAL = 3,
+  PF_COV_MATERN = 4,
+  PF_COV_MATERN32 = 5,
+  PF_COV_MATERN52 = 6,
+  PF_COV_DAMPED_OSCILLATION = 7,
+  PF_COV_GAMMA_EXPONENTIAL = 8,
+  PF_COV_CAUCHY = 9,
+  PF_COV_GENERALIZED_CAUCHY = 10,
+  PF_COV_CUBIC = 11,
+  PF_COV_WHITE_NOISE = 12
+} pf_covariance;
+
+/* stochastic.anisotropy (matrix.hh:479-493) */
+typedef enum pf_anisotropy {
+  PF_ANISO_NONE = 0,        /* ScaledIdentityMatrix, covariance.hh:18-44 */
+  PF_ANISO_AXIPARALLEL = 1, /* DiagonalMatrix, covariance.hh:49-74 */
+  PF_ANISO_GEOMETRIC = 2    /* GeneralMatrix, covariance.hh:79-138 */
+} pf_anisotropy;
+
+/* Matrix backends (matrix.hh:1652-1735 give the defaults) */
+typedef enum pf_matrix_backend {
+  PF_MATRIX_DEFAULT = -1,
+  PF_MATRIX_DCT = 0, /* DCTMatrixBackend, backends/dctmatrixbackend.hh */
+  PF_MATRIX_R2C = 1, /* R2CMatrixBackend, backends/r2cmatrixbackend.hh */
+  PF_MATRIX_DFT = 2  /* DFTMatrixBackend, backends/dftmatrixbackend.hh */
+} pf_matrix_backend;
+
+/* Field backends */
+typedef enum pf_field_backend {
+  PF_FIELD_DEFAULT = -1,
+  PF_FIELD_R2C = 0,   /* R2CFieldBackend, backends/r2cfieldbackend.hh */
+  PF_FIELD_DFT = 1,   /* DFTFieldBackend, backends/dftfieldbackend.hh */
+  PF_FIELD_DCTDST = 2 /* DCTDSTFieldBackend, backends/dctdstfieldbackend.hh */
+} pf_field_backend;
+
+/* randomField.transform (mutators.hh:126-163) */
+typedef enum pf_transform {
+  PF_TRANSFORM_NONE = 0,
+  PF_TRANSFORM_LOGNORMAL = 1,
+  PF_TRANSFORM_FOLDEDNORMAL = 2,
+  PF_TRANSFORM_SIGN = 3,
+  PF_TRANSFORM_BOXCOX = 4
+} pf_transform;
+
+/* Arithmetic of the per-realization path (spectrum, CG reductions and residuals
+ * are always FP64). */
+typedef enum pf_precision { PF_PREC_F64 = 0, PF_PREC_F32 = 1 } pf_precision;
+
+/* Eigenvalue scan after the spectrum transform (matrix.hh:266-317).
+ * CORRECTED scans every stored eigenvalue.  REFERENCE reproduces the reference
+ * exactly, including the R2C real-view scan that only inspects the first N_c/2
+ * complex entries (r2cmatrixbackend.hh:164-170 with get/set 378-400). */
+typedef enum pf_eigen_check { PF_EIGCHECK_CORRECTED = 0, PF_EIGCHECK_REFERENCE = 1 } pf_eigen_check;
+
+/* Matrix-vector product kinds (matrix.hh:1443-1646) */
+typedef enum pf_op {
+  PF_OP_MUL = 0,    /* multiplyExtended: eigenvalue lambda */
+  PF_OP_ROOT = 1,   /* multiplyRootExtended: sqrt(lambda) */
+  PF_OP_INVEXT = 2  /* multiplyInverseExtended: 1/lambda (torus inverse) */
+} pf_op;
+
+/* Where a caller buffer lives. */
+typedef enum pf_mem { PF_MEM_HOST = 0, PF_MEM_DEVICE = 1 } pf_mem;
+
+/* Field / covariance configuration: one field per Dune::ParameterTree key the
+ * reference reads on this path (fieldtraits.hh:175-186, 229; matrix.hh:268-269,
+ * 479-480, 515-519; covariance.hh:33-128, 395-396, 515-516, 711-713;
+ * mutators.hh:139-154). */
+typedef struct pf_field_desc {
+  int32_t dim;               /* 1, 2 or 3 */
+  int32_t cells[3];          /* grid.cells */
+  double extensions[3];      /* grid.extensions */
+  int32_t embedding_factor;  /* embedding.factor (default 2) */
+  int32_t periodic;          /* randomField.periodic: forces embedding factor 1 */
+  int32_t covariance;        /* pf_covariance, stochastic.covariance */
+  double variance;           /* stochastic.variance */
+  int32_t anisotropy;        /* pf_anisotropy, stochastic.anisotropy */
+  double corr_length[9];     /* stochastic.corrLength: scalar, dim-vector or dim x dim row-major */
+  double matern_nu;          /* stochastic.maternNu */
+  double exp_gamma;          /* stochastic.expGamma */
+  double cauchy_alpha;       /* stochastic.cauchyAlpha */
+  double cauchy_beta;        /* stochastic.cauchyBeta */
+  int32_t approximate;       /* embedding.approximate (default false) */
+  double threshold;          /* embedding.threshold (default 1e-14) */
+  int32_t transposed;        /* fftw.transposed: -1 = reference default */
+  int32_t matrix_backend;    /* pf_matrix_backend */
+  int32_t field_backend;     /* pf_field_backend */
+  int32_t precision;         /* pf_precision of realizations and FP32 matvecs */
+  int32_t eigen_check;       /* pf_eigen_check */
+  int32_t cg_iterations;     /* randomField.cgIterations (default 100) */
+  int32_t transform;         /* pf_transform, randomField.transform */
+  double boxcox_lambda;      /* transform.boxCoxLambda */
+} pf_field_desc;
+
+/* Eigenvalue statistics of matrix.hh:270-299 (counts and minimum). */
+typedef struct pf_eig_stats {
+  uint32_t small;    /* threshold <= value < 1e-6 */
+  uint32_t zero;     /* |value| < threshold */
+  uint32_t negative; /* value <= -threshold */
+  uint32_t pad_;
+  double smallest;   /* minimum scanned value */
+} pf_eig_stats;
+
+/* Sizes the plan resolved from the descriptor (fieldtraits.hh:217-314). */
+typedef struct pf_plan_info {
+  int32_t dim;
+  int32_t cells[3];
+  int32_t ext_cells[3];     /* T_i */
+  int32_t matrix_backend;   /* resolved pf_matrix_backend */
+  int32_t field_backend;    /* resolved pf_field_backend */
+  int32_t transposed;       /* resolved fftw.transposed */
+  int32_t precision;
+  uint64_t domain_size;     /* prod cells_i */
+  uint64_t ext_size;        /* N = prod T_i */
+  uint64_t spectrum_size;   /* stored eigenvalues: D (DCT), N_c (R2C), N (DFT) */
+  uint64_t noise_size;      /* doubles consumed per realization (reference draw order) */
+  uint64_t device_bytes;    /* device memory held by the plan */
+} pf_plan_info;
+
+/* CG options and report for pf_multiply_inverse (matrix.hh:189-206, 1315-1432). */
+typedef enum pf_cg_mode {
+  PF_CG_REFERENCE = 0, /* the reference's energy-stagnation rule and iteration cap */
+  PF_CG_RESIDUAL = 1   /* stop at ||b - A x|| / ||b|| <= tol with an FP64 true residual */
+} pf_cg_mode;
+
+typedef struct pf_cg_opts {
+  int32_t mode;            /* pf_cg_mode */
+  int32_t max_iterations;  /* 0 = desc.cg_iterations (reference) or 1000 (residual mode) */
+  double tolerance;        /* relative residual target for PF_CG_RESIDUAL (e.g. 1e-8) */
+  int32_t inner_fp32;      /* 1: inner CG matvecs in FP32 with FP64 refinement */
+  int32_t precondition;    /* 1: torus-inverse preconditioner (reference default) */
+} pf_cg_opts;
+
+typedef struct pf_cg_report {
+  int32_t iterations;        /* total inner CG iterations */
+  int32_t refinements;       /* outer FP64 residual recomputations */
+  double relative_residual;  /* final ||b - A x|| / ||b|| (FP64 matvec) */
+} pf_cg_report;
+
+typedef struct pf_plan pf_plan;
+
+/* Fills the descriptor with the reference's defaults (embedding.factor 2,
+ * threshold 1e-14, cgIterations 100, transposed default, FP64, isotropic
+ * exponential with unit variance and extensions). */
+void pf_field_desc_init(pf_field_desc* desc);
+
+/* Replaces the Matrix constructor + update() (matrix.hh:98-133) together with the
+ * size computation of RandomFieldTraits::update (fieldtraits.hh:217-314) and the
+ * default backend selection of RandomField (randomfield.hh:153-164). Allocates the
+ * plan's device buffers; no transform runs here (the spectrum is lazy, as in the
+ * reference, matrix.hh:333-334). */
+pf_status pf_plan_create(const pf_field_desc* desc, pf_plan** plan);
+void pf_plan_destroy(pf_plan* plan);
+
+/* Launches all work of the plan on `stream` (a cudaStream_t; NULL = the plan's own). */
+pf_status pf_plan_set_stream(pf_plan* plan, void* stream);
+pf_status pf_plan_get_info(const pf_plan* plan, pf_plan_info* info);
+
+/* Matrix::fillTransformedMatrix(covariance string) (matrix.hh:223-318): FP64
+ * covariance evaluation on the torus (matrix.hh:615-638), FP64 spectrum transform
+ * with the /N scaling, eigenvalue scan, clamp, and the NegativeEigenvalueError
+ * rule (PF_ERR_NEG_EIGEN unless desc.approximate). `stats` may be NULL. */
+pf_status pf_spectrum_build(pf_plan* plan, pf_eig_stats* stats);
+
+/* Copies the finalized eigenvalues (FP64) in the reference's storage layout
+ * (DCT: prod(T_i/2+1); R2C: N_c real parts; DFT: N real parts). */
+pf_status pf_spectrum_copy(pf_plan* plan, double* out, uint64_t count);
+
+/* Matrix::generateField (matrix.hh:330-421) for one realization.
+ * noise != NULL: `noise` holds info.noise_size standard-normal doubles in the
+ * reference's draw order (rand1, rand2 per stored frequency, matrix.hh:378-404),
+ * in memory `noise_mem`.  noise == NULL: the noise is drawn on the device from a
+ * counter-based generator keyed by `seed`.
+ * `out` receives prod(cells) values (double for PF_PREC_F64, float for PF_PREC_F32)
+ * in memory `out_mem`, with the descriptor's value transform applied when
+ * `apply_transform` is nonzero (RandomField::evaluate, randomfield.hh:641-651).
+ * With the DFT field backend the second (imaginary) field is cached in the plan
+ * and returned by the next call without consuming noise (matrix.hh:411-420). */
+pf_status pf_generate(pf_plan* plan, const double* noise, int32_t noise_mem, uint64_t seed,
+                      void* out, int32_t out_mem, int32_t apply_transform);
+
+/* `count` realizations keyed by seed, seed+1, ... written back to back into `out`. */
+pf_status pf_generate_batch(pf_plan* plan, uint64_t seed, int32_t count, void* out,
+                            int32_t out_mem, int32_t apply_transform);
+
+/* Matrix::operator* / multiplyRoot (matrix.hh:142-176, 1443-1573) and the torus
+ * inverse multiplyInverseExtended (matrix.hh:1587-1646).  `in` and `out` hold
+ * prod(cells) values of type `precision` (PF_PREC_F64: double, PF_PREC_F32: float);
+ * in == out is allowed. */
+pf_status pf_matvec(pf_plan* plan, int32_t op, int32_t precision, const void* in, void* out,
+                    int32_t mem);
+
+/* Matrix::multiplyInverse (matrix.hh:189-206): zero-input shortcut, torus-inverse
+ * initial guess, then the preconditioned CG of innerCG (matrix.hh:1315-1432).
+ * FP64 vectors; `opts` NULL = reference mode. */
+pf_status pf_multiply_inverse(pf_plan* plan, const double* b, double* x, int32_t mem,
+                              const pf_cg_opts* opts, pf_cg_report* report);
+
+/* ValueTransform::apply (mutators.hh:35-163) over `count` values of `precision`. */
+pf_status pf_apply_transform(pf_plan* plan, int32_t precision, void* data, uint64_t count,
+                             int32_t mem);
+
+/* Per-kernel device timing: when enabled, every launch of the plan is bracketed by
+ * CUDA events on the plan's stream and accumulated per kernel name. */
+pf_status pf_profile_enable(pf_plan* plan, int32_t enable);
+/* Writes up to `cap` entries; returns the number of kernels seen in *count. */
+typedef struct pf_kernel_time {
+  char name[48];
+  uint64_t launches;
+  double total_ms;
+  double bytes;  /* algorithmic bytes moved by all launches (reads + writes) */
+} pf_kernel_time;
+pf_status pf_profile_read(pf_plan* plan, pf_kernel_time* out, int32_t cap, int32_t* count);
+
+/* Number of kernel launches issued by this plan since creation. */
+uint64_t pf_launch_count(const pf_plan* plan);
+
+const char* pf_last_error_string(void);
+const char* pf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PARAFIELDS_B200_H */

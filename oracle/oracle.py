@@ -1,0 +1,199 @@
+"""ctypes wrapper of oracle/liboracle.so, the FP64 CPU restatement of the
+reference's circulant-embedding path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py, never by the product.  Parity with the reference
+binary is unpinned (the reference cannot be built here and its tests hold no
+golden vectors); the FFT conventions are pinned against scipy.fft.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), "parafields-core_b200"))
+import pfb200  # noqa: E402  (descriptor struct only; no CUDA library is loaded)
+
+_lib = None
+
+
+class Geom(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int), ("n", C.c_int * 3), ("T", C.c_int * 3), ("Ts", C.c_int * 3),
+        ("h", C.c_double * 3), ("ext", C.c_double * 3), ("factor", C.c_int),
+        ("matrix_backend", C.c_int), ("field_backend", C.c_int), ("transposed", C.c_int),
+        ("domain", C.c_uint64), ("N", C.c_uint64), ("Nc", C.c_uint64), ("D", C.c_uint64),
+        ("spectrum", C.c_uint64), ("noise", C.c_uint64),
+    ]
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        D = C.POINTER(pfb200.FieldDesc)
+        dp = C.POINTER(C.c_double)
+        L.oc_resolve.argtypes = [D, C.POINTER(Geom), C.c_char_p, C.c_int]
+        L.oc_covariance.argtypes = [D, dp]
+        L.oc_covariance.restype = C.c_double
+        L.oc_geometry.argtypes = [D, dp, dp]
+        L.oc_fft.argtypes = [C.c_int, dp, C.c_int]
+        L.oc_fft_axis.argtypes = [dp, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int]
+        L.oc_r2c.argtypes = [C.c_int, C.POINTER(C.c_int), dp, dp]
+        L.oc_c2r.argtypes = [C.c_int, C.POINTER(C.c_int), dp, dp]
+        L.oc_dct1.argtypes = [C.c_int, C.POINTER(C.c_int), dp]
+        L.oc_fill_matrix.argtypes = [D, dp, C.c_uint64]
+        L.oc_spectrum.argtypes = [D, dp, C.POINTER(pfb200.EigStats)]
+        L.oc_generate.argtypes = [D, dp, dp, dp, dp]
+        L.oc_matvec.argtypes = [D, dp, C.c_int, dp, dp]
+        L.oc_multiply_inverse.argtypes = [D, dp, dp, dp, C.POINTER(C.c_int)]
+        L.oc_transform.argtypes = [C.c_int, C.c_double, dp, C.c_uint64]
+        L.oc_num_threads.restype = C.c_int
+        L.oc_set_num_threads.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ints(v):
+    return (C.c_int * len(v))(*[int(x) for x in v])
+
+
+def set_threads(n):
+    lib().oc_set_num_threads(int(n))
+
+
+def num_threads():
+    return lib().oc_num_threads()
+
+
+def resolve(desc):
+    g = Geom()
+    err = C.create_string_buffer(256)
+    st = lib().oc_resolve(C.byref(desc), C.byref(g), err, 256)
+    if st:
+        raise ValueError(err.value.decode())
+    return g
+
+
+def fft(x, sign):
+    a = np.ascontiguousarray(x, dtype=np.complex128).copy()
+    lib().oc_fft(a.size, _dp(a.view(np.float64)), sign)
+    return a
+
+
+def fft_axis(x, axis_param, sign):
+    """x: numpy complex array with C-order shape (..., shape[1], shape[0]); axis in
+    parafields numbering (0 = fastest)."""
+    a = np.ascontiguousarray(x, dtype=np.complex128).copy()
+    shape = list(reversed(a.shape))
+    lib().oc_fft_axis(_dp(a.view(np.float64)), len(shape), _ints(shape), axis_param, sign)
+    return a
+
+
+def r2c(x):
+    """x: real array, C-order shape (T2, T1, T0) -> complex (T2, T1, T0//2+1)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    T = list(reversed(x.shape))
+    out = np.empty(x.shape[:-1] + (T[0] // 2 + 1,), dtype=np.complex128)
+    lib().oc_r2c(len(T), _ints(T), _dp(x), _dp(out.view(np.float64)))
+    return out
+
+
+def c2r(X, T0):
+    X = np.ascontiguousarray(X, dtype=np.complex128)
+    T = [T0] + list(reversed(X.shape[:-1]))
+    out = np.empty(X.shape[:-1] + (T0,), dtype=np.float64)
+    lib().oc_c2r(len(T), _ints(T), _dp(X.view(np.float64)), _dp(out))
+    return out
+
+
+def dct1(x):
+    a = np.ascontiguousarray(x, dtype=np.float64).copy()
+    m = list(reversed(a.shape))
+    lib().oc_dct1(len(m), _ints(m), _dp(a))
+    return a
+
+
+def covariance(desc, x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    return lib().oc_covariance(C.byref(desc), _dp(x))
+
+
+def fill_matrix(desc):
+    g = resolve(desc)
+    if g.matrix_backend == pfb200.MATRIX_DCT:
+        cells = [g.T[i] // 2 + 1 if i < g.dim else 1 for i in range(3)]
+    elif g.matrix_backend == pfb200.MATRIX_R2C:
+        cells = [2 * (g.T[0] // 2 + 1)] + [g.T[i] if i < g.dim else 1 for i in (1, 2)]
+    else:
+        cells = [g.T[i] if i < g.dim else 1 for i in range(3)]
+    out = np.empty(int(np.prod(cells)), dtype=np.float64)
+    st = lib().oc_fill_matrix(C.byref(desc), _dp(out), out.size)
+    assert st == 0, st
+    return out
+
+
+def spectrum(desc):
+    """(lambda in the reference's storage layout, stats dict, status)."""
+    g = resolve(desc)
+    lam = np.empty(g.spectrum, dtype=np.float64)
+    st = pfb200.EigStats()
+    status = lib().oc_spectrum(C.byref(desc), _dp(lam), C.byref(st))
+    return lam, st.as_dict(), status
+
+
+def generate(desc, lam, noise):
+    g = resolve(desc)
+    assert noise.size == g.noise and noise.dtype == np.float64
+    field = np.empty(g.domain, dtype=np.float64)
+    spare = np.empty(g.domain, dtype=np.float64)
+    st = lib().oc_generate(C.byref(desc), _dp(lam), _dp(np.ascontiguousarray(noise)), _dp(field),
+                           _dp(spare))
+    assert st == 0, st
+    return field, spare
+
+
+def matvec(desc, lam, op, x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    st = lib().oc_matvec(C.byref(desc), _dp(lam), op, _dp(x), _dp(out))
+    assert st == 0, st
+    return out
+
+
+def multiply_inverse(desc, lam, b):
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.empty_like(b)
+    it = C.c_int()
+    st = lib().oc_multiply_inverse(C.byref(desc), _dp(lam), _dp(b), _dp(x), C.byref(it))
+    assert st == 0, st
+    return x, it.value
+
+
+def transform(kind, v, boxcox_lambda=0.0):
+    a = np.ascontiguousarray(v, dtype=np.float64).copy()
+    k = pfb200.TRANSFORMS[kind] if isinstance(kind, str) else int(kind)
+    lib().oc_transform(k, boxcox_lambda, _dp(a), a.size)
+    return a
+
+
+def noise(seed, count):
+    """Seeded N(0,1) doubles (numpy PCG64 + its standard normal method); the same
+    buffer is fed to the oracle and to the GPU in the reference's draw order."""
+    return np.random.default_rng(seed).standard_normal(int(count))

@@ -1,0 +1,1194 @@
+// pf_capi.cu -- C ABI of the single-GPU circulant-embedding path (include/parafields_b200.h).
+//
+// One translation unit: the plan object, the pass schedules of each Matrix operation
+// and the device-side CG.  All kernels live in pf_kernels.cuh / pf_fft.cuh /
+// pf_cg.cuh; nothing here runs arithmetic on the host except the tiny CG scalars.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/parafields_b200.h"
+#include "pf_cg.cuh"
+#include "pf_kernels.cuh"
+
+using namespace pf;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+static pf_status fail(pf_status st, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return st;
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(e_ == cudaErrorMemoryAllocation ? PF_ERR_OOM : PF_ERR_CUDA, "%s: %s (%s:%d)", \
+                  #call, cudaGetErrorString(e_), __FILE__, __LINE__);                    \
+  } while (0)
+
+#define TRY(...)                   \
+  do {                             \
+    pf_status s_ = (__VA_ARGS__);  \
+    if (s_ != PF_OK) return s_;    \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// resolved geometry (RandomFieldTraits::update, fieldtraits.hh:217-314, and the
+// default Matrix selection of RandomField, randomfield.hh:153-164)
+// ---------------------------------------------------------------------------
+struct Geom {
+  int dim;
+  int n[3], T[3], Ts[3];
+  double h[3], ext[3];
+  int factor;
+  int mb, fb, transposed;
+  int T0c;
+  uint64_t domain, N, Nc, D, S, noise;
+  int C[3];  // cells of the transformed spectrum array (natural layout)
+};
+
+static pf_status resolve(const pf_field_desc* d, Geom* g) {
+  memset(g, 0, sizeof(*g));
+  if (d->dim < 1 || d->dim > 3) return fail(PF_ERR_CONFIG, "dimension must be 1, 2 or 3");
+  g->dim = d->dim;
+  g->factor = d->periodic ? 1 : d->embedding_factor;
+  if (g->factor < 1) return fail(PF_ERR_CONFIG, "embedding.factor must be positive");
+  for (int i = 0; i < 3; i++) {
+    g->n[i] = 1;
+    g->T[i] = 1;
+    g->h[i] = 1.;
+    g->ext[i] = 1.;
+  }
+  for (int i = 0; i < d->dim; i++) {
+    if (d->cells[i] < 1) return fail(PF_ERR_CONFIG, "grid.cells must be positive");
+    g->n[i] = d->cells[i];
+    g->ext[i] = d->extensions[i];
+    g->h[i] = d->extensions[i] / (double)d->cells[i];
+    g->T[i] = g->factor * d->cells[i];
+  }
+  int mb = d->matrix_backend, fb = d->field_backend;
+  if (mb < 0)
+    mb = d->dim == 1 ? PF_MATRIX_DFT
+                     : ((d->anisotropy == PF_ANISO_NONE || d->anisotropy == PF_ANISO_AXIPARALLEL) ? PF_MATRIX_DCT
+                                                                                                 : PF_MATRIX_R2C);
+  if (fb < 0) fb = d->dim == 1 ? PF_FIELD_DFT : PF_FIELD_R2C;
+  if (mb > 2 || fb > 2) return fail(PF_ERR_CONFIG, "unknown backend");
+  if (d->dim == 1 && (mb != PF_MATRIX_DFT || fb != PF_FIELD_DFT))
+    return fail(PF_ERR_CONFIG, "dim 1 requires DFTMatrixBackend and DFTFieldBackend");
+  if (fb == PF_FIELD_DFT && mb == PF_MATRIX_R2C)
+    return fail(PF_ERR_CONFIG, "R2CMatrixBackend cannot serve DFTFieldBackend");
+  if (fb == PF_FIELD_DCTDST) return fail(PF_ERR_CONFIG, "DCTDSTFieldBackend is not supported");
+  for (int i = 0; i < d->dim; i++)
+    if (mb == PF_MATRIX_DCT && (g->T[i] % 2))
+      return fail(PF_ERR_CONFIG, "DCTMatrixBackend requires an even number of extended cells per dimension");
+  if ((mb == PF_MATRIX_R2C || fb == PF_FIELD_R2C) && (g->T[0] % 2))
+    return fail(PF_ERR_CONFIG, "the R2C backends need an even number of extended cells in dimension 0");
+  g->mb = mb;
+  g->fb = fb;
+  int t = d->transposed < 0 ? (d->dim > 1) : (d->transposed != 0);
+  if (d->dim == 1) t = 0;
+  if (d->dim == 2 && (mb == PF_MATRIX_R2C || fb == PF_FIELD_R2C)) t = 0;
+  g->transposed = t;
+  for (int i = 0; i < 3; i++) g->Ts[i] = g->T[i];
+  if (t) std::swap(g->Ts[d->dim - 1], g->Ts[d->dim - 2]);
+  g->T0c = g->T[0] / 2 + 1;
+  g->domain = 1;
+  g->N = 1;
+  g->D = 1;
+  for (int i = 0; i < d->dim; i++) {
+    g->domain *= (uint64_t)g->n[i];
+    g->N *= (uint64_t)g->T[i];
+    g->D *= (uint64_t)(g->T[i] / 2 + 1);
+  }
+  g->Nc = g->N / (uint64_t)g->T[0] * (uint64_t)g->T0c;
+  g->S = mb == PF_MATRIX_DCT ? g->D : (mb == PF_MATRIX_R2C ? g->Nc : g->N);
+  g->noise = fb == PF_FIELD_R2C ? 2 * g->Nc : 2 * g->N;
+  for (int i = 0; i < 3; i++) g->C[i] = 1;
+  for (int i = 0; i < d->dim; i++)
+    g->C[i] = mb == PF_MATRIX_DCT ? g->T[i] / 2 + 1 : (mb == PF_MATRIX_R2C ? (i == 0 ? g->T0c : g->T[i]) : g->T[i]);
+  if (g->N > 0xffffffffull) return fail(PF_ERR_CONFIG, "extended domain exceeds 2^32 cells");
+  const int c = d->covariance;
+  if (c < 0 || c > PF_COV_WHITE_NOISE) return fail(PF_ERR_CONFIG, "covariance structure not known");
+  if (c == PF_COV_GAMMA_EXPONENTIAL && (d->exp_gamma < 0. || d->exp_gamma > 2.))
+    return fail(PF_ERR_CONFIG, "exponent gamma has to be between 0 and 2");
+  if (c == PF_COV_MATERN) return fail(PF_ERR_CONFIG, "general matern requires the GNU Scientific Library (gsl)");
+  if (c == PF_COV_GENERALIZED_CAUCHY) {
+    if (d->cauchy_alpha <= 0. || d->cauchy_alpha > 2.)
+      return fail(PF_ERR_CONFIG, "generalized Cauchy alpha has to be in range (0,2]");
+    if (d->cauchy_beta <= 0.) return fail(PF_ERR_CONFIG, "generalized Cauchy beta has to be positive");
+  }
+  if (c == PF_COV_CUBIC && d->dim == 3) return fail(PF_ERR_CONFIG, "cubic covariance only applicable in 1D or 2D");
+  if (d->anisotropy < 0 || d->anisotropy > 2)
+    return fail(PF_ERR_CONFIG, "stochastic.anisotropy must be \"none\", \"axiparallel\" or \"geometric\"");
+  if (d->precision != PF_PREC_F64 && d->precision != PF_PREC_F32) return fail(PF_ERR_CONFIG, "unknown precision");
+  return PF_OK;
+}
+
+// radix schedule for a pencil length (largest radices first)
+static bool make_radices(int L, Radices* r) {
+  r->n = 0;
+  int x = L;
+  while (x % 8 == 0) r->r[r->n++] = 8, x /= 8;
+  while (x % 4 == 0) r->r[r->n++] = 4, x /= 4;
+  while (x % 2 == 0) r->r[r->n++] = 2, x /= 2;
+  static const int odd[] = {3, 5, 7, 11, 13};
+  for (int p : odd)
+    while (x % p == 0) r->r[r->n++] = p, x /= p;
+  return x == 1 && r->n < 20;
+}
+
+// ---------------------------------------------------------------------------
+// plan
+// ---------------------------------------------------------------------------
+struct ProfRec {
+  const char* name;
+  cudaEvent_t e0, e1;
+  double bytes;
+};
+
+struct pf_plan {
+  pf_field_desc desc;
+  Geom g;
+  cudaStream_t stream = nullptr, own = nullptr;
+  int device = 0;
+  // spectrum (natural layout, g.S entries)
+  bool have_spec = false;
+  pf_eig_stats stats{};
+  double* lam64 = nullptr;
+  double* sq64 = nullptr;
+  float* sq32 = nullptr;
+  float* lam32 = nullptr;
+  void* fac[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  ScanOut* scan = nullptr;
+  // workspaces
+  void* ws[3] = {nullptr, nullptr, nullptr};
+  size_t ws_bytes[3] = {0, 0, 0};
+  double* noise_dev = nullptr;
+  size_t noise_cap = 0;
+  void* io_dev = nullptr;
+  size_t io_cap = 0;
+  void* io2_dev = nullptr;
+  size_t io2_cap = 0;
+  // DFT backend spare field (matrix.hh:411-420)
+  bool spare_valid = false;
+  void* spare = nullptr;
+  size_t spare_cap = 0;
+  // twiddles per (length, element size)
+  std::map<std::pair<int, int>, void*> tw;
+  // CG scratch
+  CgScratch cg;
+  // profiling
+  bool prof = false;
+  std::vector<ProfRec> recs;
+  std::vector<cudaEvent_t> evpool;
+  uint64_t launches = 0;
+  uint64_t bytes_held = 0;
+};
+
+static pf_status dalloc(pf_plan* P, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(PF_ERR_OOM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+  }
+  P->bytes_held += bytes;
+  return PF_OK;
+}
+
+static void dfree(pf_plan* P, void** p, size_t bytes) {
+  if (*p) {
+    cudaFree(*p);
+    P->bytes_held -= bytes;
+    *p = nullptr;
+  }
+}
+
+static pf_status ensure(pf_plan* P, void** p, size_t* cap, size_t bytes) {
+  if (*cap >= bytes && *p) return PF_OK;
+  dfree(P, p, *cap);
+  *cap = 0;
+  TRY(dalloc(P, p, bytes));
+  *cap = bytes;
+  return PF_OK;
+}
+
+static pf_status workspace(pf_plan* P, int i, size_t bytes, void** out) {
+  TRY(ensure(P, &P->ws[i], &P->ws_bytes[i], bytes));
+  *out = P->ws[i];
+  return PF_OK;
+}
+
+template <typename T>
+static pf_status twiddles(pf_plan* P, int L, const cx<T>** out) {
+  auto key = std::make_pair(L, (int)sizeof(T));
+  auto it = P->tw.find(key);
+  if (it != P->tw.end()) {
+    *out = (const cx<T>*)it->second;
+    return PF_OK;
+  }
+  std::vector<cx<T>> h(L);
+  for (int m = 0; m < L; m++) {
+    long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)L;
+    h[m].x = (T)cosl(a);
+    h[m].y = (T)-sinl(a);
+  }
+  void* d = nullptr;
+  size_t bytes = sizeof(cx<T>) * (size_t)L;
+  TRY(dalloc(P, &d, bytes));
+  CK(cudaMemcpy(d, h.data(), bytes, cudaMemcpyHostToDevice));
+  P->tw[key] = d;
+  *out = (const cx<T>*)d;
+  return PF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+static pf_status prof_begin(pf_plan* P, const char* name, double bytes, ProfRec* rec) {
+  rec->name = name;
+  rec->bytes = bytes;
+  rec->e0 = rec->e1 = nullptr;
+  if (!P->prof) return PF_OK;
+  for (int k = 0; k < 2; k++) {
+    cudaEvent_t e;
+    if (!P->evpool.empty()) {
+      e = P->evpool.back();
+      P->evpool.pop_back();
+    } else {
+      CK(cudaEventCreate(&e));
+    }
+    (k ? rec->e1 : rec->e0) = e;
+  }
+  CK(cudaEventRecord(rec->e0, P->stream));
+  return PF_OK;
+}
+
+static pf_status prof_end(pf_plan* P, ProfRec* rec) {
+  P->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(PF_ERR_CUDA, "launch of %s failed: %s", rec->name, cudaGetErrorString(e));
+  if (!P->prof) return PF_OK;
+  CK(cudaEventRecord(rec->e1, P->stream));
+  P->recs.push_back(*rec);
+  return PF_OK;
+}
+
+static int pow2_floor(int x) {
+  int p = 1;
+  while (p * 2 <= x) p *= 2;
+  return p;
+}
+
+// pencils per tile: two shared buffers of B pencils within ~64 KB
+static void tile_params(int L, int elem, bool contig, PassArgs* a) {
+  const int pitch = contig ? L + 1 : L;
+  int per = 2 * pitch * elem;
+  int B = std::max(1, pow2_floor(std::max(1, 65536 / per)));
+  B = std::min(B, 16);
+  if (!contig && B < 4 && per * 4 <= 160 * 1024) B = 4;
+  if (!contig && B < 2 && per * 2 <= 200 * 1024) B = 2;
+  a->B = B;
+  a->pitch = pitch;
+}
+
+static size_t smem_of(const PassArgs& a, bool contig, int elem) {
+  return (size_t)2 * a.B * (contig ? a.pitch : a.L) * elem;
+}
+
+template <typename K>
+static pf_status set_smem(K kernel, size_t smem) {
+  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return PF_OK;
+}
+
+// complex pencil pass along a strided axis or along contiguous rows
+template <typename T, bool CONTIG, class Ld, class Mid, class St>
+static pf_status run_pass(pf_plan* P, const char* name, int L, int Lout, long long npencil, long long nouter,
+                          int sign, int sign2, Ld ld, Mid mid, St st, double bytes) {
+  PassArgs a{};
+  a.L = L;
+  a.Lout = Lout;
+  a.npencil = npencil;
+  a.nouter = nouter;
+  a.sign = sign;
+  a.sign2 = sign2;
+  if (!make_radices(L, &a.rad)) return fail(PF_ERR_CONFIG, "transform length %d has a prime factor above 13", L);
+  tile_params(L, (int)sizeof(cx<T>), CONTIG, &a);
+  const cx<T>* tw = nullptr;
+  TRY(twiddles<T>(P, L, &tw));
+  const size_t smem = smem_of(a, CONTIG, (int)sizeof(cx<T>));
+  if (smem > 227 * 1024) return fail(PF_ERR_CONFIG, "pencil of length %d does not fit in shared memory", L);
+  auto kern = k_pass<T, CONTIG, Ld, Mid, St>;
+  TRY(set_smem(kern, smem));
+  long long grid = CONTIG ? (npencil + a.B - 1) / a.B : ((npencil + a.B - 1) / a.B) * nouter;
+  if (grid <= 0) return PF_OK;
+  ProfRec rec;
+  TRY(prof_begin(P, name, bytes, &rec));
+  kern<<<(unsigned)grid, kThreads, smem, P->stream>>>(a, tw, ld, mid, st);
+  return prof_end(P, &rec);
+}
+
+// real-data passes along dimension 0: rows of T0 = 2L reals <-> L+1 complex
+template <typename T, bool R2C, class Ld, class St>
+static pf_status run_real_pass(pf_plan* P, const char* name, int T0, int Lout, long long rows, Ld ld, St st,
+                               double bytes) {
+  PassArgs a{};
+  a.L = T0 / 2;
+  a.Lout = Lout;
+  a.npencil = rows;
+  a.nouter = 1;
+  a.sign = R2C ? -1 : 1;
+  if (!make_radices(a.L, &a.rad)) return fail(PF_ERR_CONFIG, "transform length %d has a prime factor above 13", T0);
+  tile_params(a.L, (int)sizeof(cx<T>), true, &a);
+  const cx<T>* tw = nullptr;
+  const cx<T>* twT = nullptr;
+  TRY(twiddles<T>(P, a.L, &tw));
+  TRY(twiddles<T>(P, T0, &twT));
+  const size_t smem = smem_of(a, true, (int)sizeof(cx<T>));
+  if (smem > 227 * 1024) return fail(PF_ERR_CONFIG, "row of length %d does not fit in shared memory", T0);
+  long long grid = (rows + a.B - 1) / a.B;
+  if (grid <= 0) return PF_OK;
+  ProfRec rec;
+  if constexpr (R2C) {
+    auto kern = k_r2c<T, Ld, St>;
+    TRY(set_smem(kern, smem));
+    TRY(prof_begin(P, name, bytes, &rec));
+    kern<<<(unsigned)grid, kThreads, smem, P->stream>>>(a, tw, twT, ld, st);
+  } else {
+    auto kern = k_c2r<T, Ld, St>;
+    TRY(set_smem(kern, smem));
+    TRY(prof_begin(P, name, bytes, &rec));
+    kern<<<(unsigned)grid, kThreads, smem, P->stream>>>(a, tw, twT, ld, st);
+  }
+  return prof_end(P, &rec);
+}
+
+// capacity (bytes) of the workspace holding p: the bound every access is checked against
+static size_t cap_of(const pf_plan* P, const void* p) {
+  for (int i = 0; i < 3; i++)
+    if (p == P->ws[i]) return P->ws_bytes[i];
+  return 0;
+}
+
+template <typename S>
+static ArrLoad<S> arr_load(const pf_plan* P, const void* p, long long jstride, long long ostride, long long rowstride,
+                           int Lin) {
+  ArrLoad<S> l;
+  l.ptr = (const S*)p;
+  l.n = (long long)(cap_of(P, p) / sizeof(S));
+  l.jstride = jstride;
+  l.ostride = ostride;
+  l.rowstride = rowstride;
+  l.Lin = Lin;
+  return l;
+}
+
+template <typename S>
+static ArrStore<S> arr_store(const pf_plan* P, void* p, long long jstride, long long ostride, long long rowstride) {
+  ArrStore<S> s;
+  s.ptr = (S*)p;
+  s.n = (long long)(cap_of(P, p) / sizeof(S));
+  s.jstride = jstride;
+  s.ostride = ostride;
+  s.rowstride = rowstride;
+  return s;
+}
+
+static unsigned grid_for(uint64_t n) {
+  uint64_t g = (n + kThreads - 1) / kThreads;
+  if (g > 148ull * 16) g = 148ull * 16;
+  if (g == 0) g = 1;
+  return (unsigned)g;
+}
+
+// ---------------------------------------------------------------------------
+// spectrum: fillTransformedMatrix (matrix.hh:223-318)
+// ---------------------------------------------------------------------------
+static CovParams cov_params(const pf_field_desc* d, const Geom& g) {
+  CovParams c{};
+  c.dim = g.dim;
+  c.cov = d->covariance;
+  c.aniso = d->anisotropy;
+  for (int i = 0; i < 3; i++) {
+    c.T[i] = g.T[i];
+    c.h[i] = g.h[i];
+    c.half[i] = 0.5 * g.ext[i] * (double)g.factor;
+    c.wrap[i] = g.ext[i] * (double)g.factor;
+  }
+  const double* cl = d->corr_length;
+  if (d->anisotropy == PF_ANISO_NONE) {
+    c.geo[0] = 1. / cl[0];  // covariance.hh:33-37
+  } else if (d->anisotropy == PF_ANISO_AXIPARALLEL) {
+    for (int i = 0; i < g.dim; i++) c.geo[i] = 1. / cl[i];  // covariance.hh:62-67
+  } else {  // cofactor inverse, covariance.hh:94-128
+    double* m = c.geo;
+    if (g.dim == 3) {
+      m[0] = cl[4] * cl[8] - cl[5] * cl[7];
+      m[1] = cl[2] * cl[7] - cl[1] * cl[8];
+      m[2] = cl[1] * cl[5] - cl[2] * cl[4];
+      m[3] = cl[5] * cl[6] - cl[3] * cl[8];
+      m[4] = cl[0] * cl[8] - cl[2] * cl[6];
+      m[5] = cl[2] * cl[3] - cl[0] * cl[5];
+      m[6] = cl[3] * cl[7] - cl[4] * cl[6];
+      m[7] = cl[1] * cl[6] - cl[0] * cl[7];
+      m[8] = cl[0] * cl[4] - cl[1] * cl[3];
+      const double det = cl[0] * (cl[4] * cl[8] - cl[5] * cl[7]) - cl[1] * (cl[3] * cl[8] - cl[5] * cl[6]) +
+                         cl[2] * (cl[3] * cl[7] - cl[4] * cl[6]);
+      for (int i = 0; i < 9; i++) m[i] /= det;
+    } else if (g.dim == 2) {
+      m[0] = cl[3];
+      m[1] = -cl[1];
+      m[2] = -cl[2];
+      m[3] = cl[0];
+      const double det = cl[0] * cl[3] - cl[1] * cl[2];
+      for (int i = 0; i < 4; i++) m[i] /= det;
+    } else {
+      m[0] = 1. / cl[0];
+    }
+  }
+  c.variance = d->variance;
+  if (d->covariance == PF_COV_GAMMA_EXPONENTIAL) c.p0 = d->exp_gamma;
+  if (d->covariance == PF_COV_GENERALIZED_CAUCHY) {
+    c.p0 = d->cauchy_alpha;
+    c.p1 = d->cauchy_beta;
+  }
+  return c;
+}
+
+static pf_status spectrum_alloc(pf_plan* P) {
+  const uint64_t S = P->g.S;
+  if (!P->lam64) {
+    TRY(dalloc(P, (void**)&P->lam64, S * 8));
+    TRY(dalloc(P, (void**)&P->sq64, S * 8));
+    TRY(dalloc(P, (void**)&P->sq32, S * 4));
+    TRY(dalloc(P, (void**)&P->lam32, S * 4));
+    TRY(dalloc(P, (void**)&P->scan, sizeof(ScanOut)));
+  }
+  return PF_OK;
+}
+
+static pf_status build_spectrum(pf_plan* P) {
+  const Geom& g = P->g;
+  const pf_field_desc* d = &P->desc;
+  TRY(spectrum_alloc(P));
+  for (int a = 0; a < 2; a++)
+    for (int o = 0; o < 3; o++)
+      if (P->fac[a][o]) {
+        cudaFree(P->fac[a][o]);
+        P->bytes_held -= g.S * (a == 0 ? 8 : 4);
+        P->fac[a][o] = nullptr;
+      }
+  CovRowLoad cl;
+  cl.c = cov_params(d, g);
+  const int dim = g.dim;
+  void *A = nullptr, *Bw = nullptr;
+  double2* spec = nullptr;
+  const uint64_t full = g.mb == PF_MATRIX_DFT ? g.N : g.Nc;
+  TRY(workspace(P, 0, full * sizeof(double2), &A));
+  TRY(workspace(P, 1, full * sizeof(double2), &Bw));
+  if (g.mb == PF_MATRIX_DCT || g.mb == PF_MATRIX_R2C) {
+    const bool dct = g.mb == PF_MATRIX_DCT;
+    const int T0c = g.T0c;
+    const long long rows = (long long)(g.N / (uint64_t)g.T[0]);
+    // dimension 0: covariance evaluation fused into the R2C load
+    TRY((run_real_pass<double, true>(P, "spec_r2c_cov", g.T[0], T0c, rows, cl,
+                                     arr_store<double2>(P, A, 1, 0, T0c), rows * T0c * 16.0)));
+    spec = (double2*)A;
+    if (dim >= 2) {
+      const int L1 = g.T[1], L1o = dct ? g.T[1] / 2 + 1 : g.T[1];
+      const long long outer = dim == 3 ? g.T[2] : 1;
+      TRY((run_pass<double, false>(P, "spec_c2c_d1", L1, L1o, T0c, outer, -1, -1,
+                                   arr_load<double2>(P, A, T0c, (long long)T0c * L1, 1, L1), NoMid(),
+                                   arr_store<double2>(P, Bw, T0c, (long long)T0c * L1o, 1),
+                                   (double)T0c * outer * (L1 + L1o) * 16.0)));
+      spec = (double2*)Bw;
+      if (dim == 3) {
+        const int L2 = g.T[2], L2o = dct ? g.T[2] / 2 + 1 : g.T[2];
+        const long long inner = (long long)T0c * L1o;
+        TRY((run_pass<double, false>(P, "spec_c2c_d2", L2, L2o, inner, 1, -1, -1,
+                                     arr_load<double2>(P, Bw, inner, 0, 1, L2), NoMid(),
+                                     arr_store<double2>(P, A, inner, 0, 1), (double)inner * (L2 + L2o) * 16.0)));
+        spec = (double2*)A;
+      }
+    }
+  } else {  // DFT matrix: complex torus, every axis complex (dftmatrixbackend.hh:209-238)
+    const long long rows = (long long)(g.N / (uint64_t)g.T[0]);
+    TRY((run_pass<double, true>(P, "spec_c2c_d0", g.T[0], g.T[0], rows, 1, -1, -1, cl, NoMid(),
+                                arr_store<double2>(P, A, 1, 0, g.T[0]), rows * g.T[0] * 16.0)));
+    spec = (double2*)A;
+    void* src = A;
+    void* dst = Bw;
+    long long inner = g.T[0];
+    for (int ax = 1; ax < dim; ax++) {
+      const int L = g.T[ax];
+      long long outer = (long long)(g.N / (uint64_t)inner / (uint64_t)L);
+      TRY((run_pass<double, false>(P, ax == 1 ? "spec_c2c_d1" : "spec_c2c_d2", L, L, inner, outer, -1, -1,
+                                   arr_load<double2>(P, src, inner, inner * L, 1, L), NoMid(),
+                                   arr_store<double2>(P, dst, inner, inner * L, 1), (double)g.N * 32.0)));
+      spec = (double2*)dst;
+      std::swap(src, dst);
+      inner *= L;
+    }
+  }
+  // eigenvalue scan, clamp, square roots
+  CK(cudaMemsetAsync(P->scan, 0, sizeof(ScanOut), P->stream));
+  ScanArgs sa{};
+  sa.spec = spec;
+  for (int i = 0; i < 3; i++) {
+    sa.C[i] = g.C[i];
+    sa.Ts[i] = g.Ts[i];
+  }
+  sa.transposed = g.transposed;
+  sa.dim = dim;
+  sa.faithful = (g.mb == PF_MATRIX_R2C && d->eigen_check == PF_EIGCHECK_REFERENCE) ? 1 : 0;
+  sa.count = g.S;
+  sa.N = (double)(unsigned int)g.N;
+  sa.threshold = d->threshold;
+  sa.lam = P->lam64;
+  sa.sq64 = P->sq64;
+  sa.sq32 = P->sq32;
+  sa.lam32 = P->lam32;
+  sa.out = P->scan;
+  {
+    ProfRec rec;
+    TRY(prof_begin(P, "spec_scan", g.S * (16.0 + 24.0), &rec));
+    k_scan<<<grid_for(g.S), kThreads, 0, P->stream>>>(sa);
+    TRY(prof_end(P, &rec));
+  }
+  ScanOut so;
+  CK(cudaMemcpyAsync(&so, P->scan, sizeof(so), cudaMemcpyDeviceToHost, P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  P->stats.small = so.small;
+  P->stats.zero = so.zero;
+  P->stats.negative = so.negative;
+  P->stats.pad_ = 0;
+  unsigned long long k = so.minkey;
+  unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  double mn;
+  memcpy(&mn, &b, 8);
+  P->stats.smallest = mn;
+  // release the FP64 spectrum workspaces: they are the largest buffers of the plan
+  dfree(P, &P->ws[0], P->ws_bytes[0]);
+  P->ws_bytes[0] = 0;
+  dfree(P, &P->ws[1], P->ws_bytes[1]);
+  P->ws_bytes[1] = 0;
+  if (P->stats.negative > 0 && !d->approximate) {
+    P->have_spec = false;
+    return fail(PF_ERR_NEG_EIGEN, "negative eigenvalues in covariance matrix");
+  }
+  P->have_spec = true;
+  return PF_OK;
+}
+
+// reads and clears the kernels' bounds-violation flag (synchronizes the stream)
+static pf_status check_bounds(pf_plan* P, pf_status st) {
+  unsigned int flag = 0;
+  CK(cudaMemcpyFromSymbolAsync(&flag, g_bounds_error, sizeof(flag), 0, cudaMemcpyDeviceToHost, P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  if (flag) {
+    const unsigned int zero = 0;
+    CK(cudaMemcpyToSymbolAsync(g_bounds_error, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, P->stream));
+    CK(cudaStreamSynchronize(P->stream));
+    return fail(PF_ERR_CUDA, "internal error: a kernel computed an index outside its buffer (access skipped)");
+  }
+  return st;
+}
+
+static pf_status ensure_spectrum(pf_plan* P) {
+  if (P->have_spec) return PF_OK;
+  return build_spectrum(P);
+}
+
+template <typename T>
+static pf_status factor_array(pf_plan* P, int op, const T** out) {
+  const int a = sizeof(T) == 8 ? 0 : 1;
+  if (!P->fac[a][op]) {
+    TRY(dalloc(P, &P->fac[a][op], P->g.S * sizeof(T)));
+    ProfRec rec;
+    TRY(prof_begin(P, "factors", P->g.S * (8.0 + sizeof(T)), &rec));
+    k_factors<T><<<grid_for(P->g.S), kThreads, 0, P->stream>>>(P->lam64, P->g.S, 1.0 / (double)P->g.N, op,
+                                                               (T*)P->fac[a][op]);
+    TRY(prof_end(P, &rec));
+  }
+  *out = (const T*)P->fac[a][op];
+  return PF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// generation: generateField (matrix.hh:330-421)
+// ---------------------------------------------------------------------------
+template <typename T, typename S>
+static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* out, int transform) {
+  const Geom& g = P->g;
+  const int T0c = g.T0c;
+  R2CNoise nz{};
+  nz.dim = g.dim;
+  for (int i = 0; i < 3; i++) nz.ext[i] = g.T[i];
+  nz.T0c = T0c;
+  nz.transposed = g.transposed;
+  nz.dct = g.mb == PF_MATRIX_DCT ? 1 : (g.mb == PF_MATRIX_DFT ? 2 : 0);
+  nz.D0 = g.T[0] / 2 + 1;
+  nz.D1 = g.T[1] / 2 + 1;
+  nz.sq = sizeof(T) == 8 ? (const void*)P->sq64 : (const void*)P->sq32;
+  nz.noise = noise_dev;
+  nz.seed = seed;
+  nz.nsq = (long long)g.S;
+  nz.nnoise = (long long)g.noise;
+  FieldRowStore<S> fs{out, g.n[0], transform, P->desc.boxcox_lambda, (long long)g.domain};
+  const double e = sizeof(cx<T>);
+  const double noise_b = noise_dev ? 16.0 : 0.0;
+  const double lam_b = sizeof(T);
+  if (g.dim == 2) {
+    void* W1 = nullptr;
+    TRY(workspace(P, 0, sizeof(cx<T>) * (size_t)T0c * g.n[1], &W1));
+    // dimension 1 first: noise scaling fused into the load, output pruned to n1
+    TRY((run_pass<T, false>(P, "gen_noise_d1", g.T[1], g.n[1], T0c, 1, +1, +1, nz, NoMid(),
+                            arr_store<cx<T>>(P, W1, T0c, 0, 1),
+                            (double)T0c * g.T[1] * (noise_b + lam_b) + (double)T0c * g.n[1] * e)));
+    TRY((run_real_pass<T, false>(P, "gen_c2r_d0", g.T[0], g.n[0], g.n[1], arr_load<cx<T>>(P, W1, 1, 0, T0c, T0c), fs,
+                                 (double)g.n[1] * (T0c * e + g.n[0] * sizeof(S)))));
+    return PF_OK;
+  }
+  void *W1 = nullptr, *W2 = nullptr;
+  TRY(workspace(P, 0, sizeof(cx<T>) * (size_t)T0c * g.T[1] * g.n[2], &W1));
+  TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)T0c * g.n[1] * g.n[2], &W2));
+  const long long inner = (long long)T0c * g.T[1];
+  TRY((run_pass<T, false>(P, "gen_noise_d2", g.T[2], g.n[2], inner, 1, +1, +1, nz, NoMid(),
+                          arr_store<cx<T>>(P, W1, inner, 0, 1),
+                          (double)inner * g.T[2] * (noise_b + lam_b) + (double)inner * g.n[2] * e)));
+  TRY((run_pass<T, false>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, g.n[2], +1, +1,
+                          arr_load<cx<T>>(P, W1, T0c, inner, 1, g.T[1]), NoMid(),
+                          arr_store<cx<T>>(P, W2, T0c, (long long)T0c * g.n[1], 1),
+                          (double)T0c * g.n[2] * (g.T[1] + g.n[1]) * e)));
+  TRY((run_real_pass<T, false>(P, "gen_c2r_d0", g.T[0], g.n[0], (long long)g.n[1] * g.n[2],
+                               arr_load<cx<T>>(P, W2, 1, 0, T0c, T0c), fs,
+                               (double)g.n[1] * g.n[2] * (T0c * e + g.n[0] * sizeof(S)))));
+  return PF_OK;
+}
+
+// DFT field backend: complex noise on the whole torus, backward c2c on every axis,
+// Re -> field, Im -> spare field (dftfieldbackend.hh:186-280, 380-446)
+template <typename T, typename S>
+static pf_status gen_dft(pf_plan* P, const double* noise_dev, uint64_t seed, S* out, S* spare, int transform) {
+  const Geom& g = P->g;
+  DFTNoise nz{};
+  nz.dim = g.dim;
+  for (int i = 0; i < 3; i++) {
+    nz.ext[i] = g.T[i];
+    nz.Ts[i] = g.Ts[i];
+  }
+  nz.transposed = g.transposed;
+  nz.mat = g.mb == PF_MATRIX_DCT ? 0 : 2;
+  nz.sq = sizeof(T) == 8 ? (const void*)P->sq64 : (const void*)P->sq32;
+  nz.noise = noise_dev;
+  nz.seed = seed;
+  nz.nsq = (long long)g.S;
+  nz.nnoise = (long long)g.noise;
+  SplitStore<S> ss{out, spare, g.n[0], transform, P->desc.boxcox_lambda, (long long)g.domain};
+  const double e = sizeof(cx<T>);
+  if (g.dim == 1) {
+    return run_pass<T, true>(P, "gen_dft_d0", g.T[0], g.n[0], 1, 1, +1, +1, nz, NoMid(), ss,
+                             (double)g.T[0] * (16.0 + sizeof(T)) + 2.0 * g.n[0] * sizeof(S));
+  }
+  void *W1 = nullptr, *W2 = nullptr;
+  const int last = g.dim - 1;
+  const long long inner = (long long)(g.N / (uint64_t)g.T[last]);
+  TRY(workspace(P, 0, sizeof(cx<T>) * (size_t)inner * g.n[last], &W1));
+  TRY(run_pass<T, false>(P, "gen_dft_noise", g.T[last], g.n[last], inner, 1, +1, +1, nz, NoMid(),
+                         arr_store<cx<T>>(P, W1, inner, 0, 1), (double)inner * (g.T[last] * 16.0 + g.n[last] * e)));
+  void* cur = W1;
+  if (g.dim == 3) {
+    TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)g.T[0] * g.n[1] * g.n[2], &W2));
+    TRY((run_pass<T, false>(P, "gen_dft_d1", g.T[1], g.n[1], g.T[0], g.n[2], +1, +1,
+                            arr_load<cx<T>>(P, W1, g.T[0], (long long)g.T[0] * g.T[1], 1, g.T[1]), NoMid(),
+                            arr_store<cx<T>>(P, W2, g.T[0], (long long)g.T[0] * g.n[1], 1),
+                            (double)g.T[0] * g.n[2] * (g.T[1] + g.n[1]) * e)));
+    cur = W2;
+  }
+  const long long rows = g.dim == 3 ? (long long)g.n[1] * g.n[2] : g.n[1];
+  return run_pass<T, true>(P, "gen_dft_d0", g.T[0], g.n[0], rows, 1, +1, +1,
+                           arr_load<cx<T>>(P, cur, 1, 0, g.T[0], g.T[0]), NoMid(), ss,
+                           (double)rows * (g.T[0] * e + 2.0 * g.n[0] * sizeof(S)));
+}
+
+// ---------------------------------------------------------------------------
+// matvecs: multiplyExtended / Root / InverseExtended (matrix.hh:1443-1646)
+// ---------------------------------------------------------------------------
+template <typename T>
+static MultMid mult_mid(pf_plan* P, const T* fac) {
+  const Geom& g = P->g;
+  MultMid m{};
+  m.dim = g.dim;
+  for (int i = 0; i < 3; i++) m.ext[i] = g.T[i];
+  m.C0 = g.fb == PF_FIELD_R2C ? g.T0c : g.T[0];
+  m.layout = g.mb == PF_MATRIX_DCT ? 0 : (g.mb == PF_MATRIX_R2C ? 1 : 2);
+  m.LC0 = g.mb == PF_MATRIX_R2C ? g.T0c : g.T[0];
+  m.D0 = g.T[0] / 2 + 1;
+  m.D1 = g.T[1] / 2 + 1;
+  m.axis = g.dim - 1;
+  m.fac = fac;
+  m.nfac = (long long)g.S;
+  return m;
+}
+
+template <typename T, typename S>
+static pf_status matvec_r2c(pf_plan* P, int op, const S* in, S* out) {
+  const Geom& g = P->g;
+  const T* fac = nullptr;
+  TRY(factor_array<T>(P, op, &fac));
+  MultMid mid = mult_mid<T>(P, fac);
+  const int T0c = g.T0c;
+  const double e = sizeof(cx<T>);
+  const double lb = sizeof(T);
+  FieldRowLoad<S> fl{in, g.n[0], (long long)g.domain};
+  FieldRowStore<S> fs{out, g.n[0], 0, 0.0, (long long)g.domain};
+  if (g.dim == 2) {
+    void* X1 = nullptr;
+    TRY(workspace(P, 2, sizeof(cx<T>) * (size_t)T0c * g.n[1], &X1));
+    TRY((run_real_pass<T, true>(P, "mv_r2c_d0", g.T[0], T0c, g.n[1], fl, arr_store<cx<T>>(P, X1, 1, 0, T0c),
+                                (double)g.n[1] * (g.n[0] * sizeof(S) + T0c * e))));
+    TRY((run_pass<T, false>(P, "mv_fused_d1", g.T[1], g.n[1], T0c, 1, -1, +1, arr_load<cx<T>>(P, X1, T0c, 0, 1, g.n[1]),
+                            mid, arr_store<cx<T>>(P, X1, T0c, 0, 1),
+                            (double)T0c * (2.0 * g.n[1] * e + g.T[1] * lb))));
+    return run_real_pass<T, false>(P, "mv_c2r_d0", g.T[0], g.n[0], g.n[1], arr_load<cx<T>>(P, X1, 1, 0, T0c, T0c), fs,
+                                   (double)g.n[1] * (T0c * e + g.n[0] * sizeof(S)));
+  }
+  void *X1 = nullptr, *X2 = nullptr;
+  TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)T0c * g.n[1] * g.n[2], &X1));
+  TRY(workspace(P, 2, sizeof(cx<T>) * (size_t)T0c * g.T[1] * g.n[2], &X2));
+  const long long rows = (long long)g.n[1] * g.n[2];
+  const long long in1 = (long long)T0c * g.T[1];
+  TRY((run_real_pass<T, true>(P, "mv_r2c_d0", g.T[0], T0c, rows, fl, arr_store<cx<T>>(P, X1, 1, 0, T0c),
+                              (double)rows * (g.n[0] * sizeof(S) + T0c * e))));
+  TRY((run_pass<T, false>(P, "mv_c2c_d1", g.T[1], g.T[1], T0c, g.n[2], -1, -1,
+                          arr_load<cx<T>>(P, X1, T0c, (long long)T0c * g.n[1], 1, g.n[1]), NoMid(),
+                          arr_store<cx<T>>(P, X2, T0c, in1, 1), (double)T0c * g.n[2] * (g.n[1] + g.T[1]) * e)));
+  TRY((run_pass<T, false>(P, "mv_fused_d2", g.T[2], g.n[2], in1, 1, -1, +1, arr_load<cx<T>>(P, X2, in1, 0, 1, g.n[2]),
+                          mid, arr_store<cx<T>>(P, X2, in1, 0, 1), (double)in1 * (2.0 * g.n[2] * e + g.T[2] * lb))));
+  TRY((run_pass<T, false>(P, "mv_c2c_d1i", g.T[1], g.n[1], T0c, g.n[2], +1, +1,
+                          arr_load<cx<T>>(P, X2, T0c, in1, 1, g.T[1]), NoMid(),
+                          arr_store<cx<T>>(P, X1, T0c, (long long)T0c * g.n[1], 1),
+                          (double)T0c * g.n[2] * (g.n[1] + g.T[1]) * e)));
+  return run_real_pass<T, false>(P, "mv_c2r_d0", g.T[0], g.n[0], rows, arr_load<cx<T>>(P, X1, 1, 0, T0c, T0c), fs,
+                                 (double)rows * (T0c * e + g.n[0] * sizeof(S)));
+}
+
+// DFT field backend matvec: complex embedding, c2c on every axis, Re extraction
+template <typename T, typename S>
+static pf_status matvec_dft(pf_plan* P, int op, const S* in, S* out) {
+  const Geom& g = P->g;
+  const T* fac = nullptr;
+  TRY(factor_array<T>(P, op, &fac));
+  MultMid mid = mult_mid<T>(P, fac);
+  const double e = sizeof(cx<T>);
+  FieldComplexLoad<S> fl{in, g.n[0], (long long)g.domain};
+  SplitStore<S> ss{out, nullptr, g.n[0], 0, 0.0, (long long)g.domain};
+  if (g.dim == 1)
+    return run_pass<T, true>(P, "mv_dft_fused_d0", g.T[0], g.n[0], 1, 1, -1, +1, fl, mid, ss,
+                             (double)g.T[0] * sizeof(T) + 2.0 * g.n[0] * sizeof(S));
+  const long long rows = (long long)(g.domain / (uint64_t)g.n[0]);
+  void *X1 = nullptr, *X2 = nullptr;
+  if (g.dim == 2) {
+    TRY(workspace(P, 2, sizeof(cx<T>) * (size_t)g.T[0] * g.n[1], &X1));
+    TRY((run_pass<T, true>(P, "mv_dft_d0", g.T[0], g.T[0], rows, 1, -1, -1, fl, NoMid(),
+                           arr_store<cx<T>>(P, X1, 1, 0, g.T[0]), (double)rows * (g.n[0] * sizeof(S) + g.T[0] * e))));
+    TRY((run_pass<T, false>(P, "mv_dft_fused_d1", g.T[1], g.n[1], g.T[0], 1, -1, +1,
+                            arr_load<cx<T>>(P, X1, g.T[0], 0, 1, g.n[1]), mid, arr_store<cx<T>>(P, X1, g.T[0], 0, 1),
+                            (double)g.T[0] * 2.0 * g.n[1] * e)));
+    return run_pass<T, true>(P, "mv_dft_d0i", g.T[0], g.n[0], rows, 1, +1, +1,
+                             arr_load<cx<T>>(P, X1, 1, 0, g.T[0], g.T[0]), NoMid(), ss,
+                             (double)rows * (g.T[0] * e + g.n[0] * sizeof(S)));
+  }
+  const long long in1 = (long long)g.T[0] * g.T[1];
+  TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)g.T[0] * g.n[1] * g.n[2], &X1));
+  TRY(workspace(P, 2, sizeof(cx<T>) * (size_t)in1 * g.n[2], &X2));
+  TRY((run_pass<T, true>(P, "mv_dft_d0", g.T[0], g.T[0], rows, 1, -1, -1, fl, NoMid(),
+                         arr_store<cx<T>>(P, X1, 1, 0, g.T[0]), (double)rows * (g.n[0] * sizeof(S) + g.T[0] * e))));
+  TRY((run_pass<T, false>(P, "mv_dft_d1", g.T[1], g.T[1], g.T[0], g.n[2], -1, -1,
+                          arr_load<cx<T>>(P, X1, g.T[0], (long long)g.T[0] * g.n[1], 1, g.n[1]), NoMid(),
+                          arr_store<cx<T>>(P, X2, g.T[0], in1, 1), (double)g.T[0] * g.n[2] * (g.n[1] + g.T[1]) * e)));
+  TRY((run_pass<T, false>(P, "mv_dft_fused_d2", g.T[2], g.n[2], in1, 1, -1, +1, arr_load<cx<T>>(P, X2, in1, 0, 1, g.n[2]),
+                          mid, arr_store<cx<T>>(P, X2, in1, 0, 1), (double)in1 * 2.0 * g.n[2] * e)));
+  TRY((run_pass<T, false>(P, "mv_dft_d1i", g.T[1], g.n[1], g.T[0], g.n[2], +1, +1,
+                          arr_load<cx<T>>(P, X2, g.T[0], in1, 1, g.T[1]), NoMid(),
+                          arr_store<cx<T>>(P, X1, g.T[0], (long long)g.T[0] * g.n[1], 1),
+                          (double)g.T[0] * g.n[2] * (g.n[1] + g.T[1]) * e)));
+  return run_pass<T, true>(P, "mv_dft_d0i", g.T[0], g.n[0], rows, 1, +1, +1,
+                           arr_load<cx<T>>(P, X1, 1, 0, g.T[0], g.T[0]), NoMid(), ss,
+                           (double)rows * (g.T[0] * e + g.n[0] * sizeof(S)));
+}
+
+template <typename T, typename S>
+static pf_status matvec_dev(pf_plan* P, int op, const S* in, S* out) {
+  if (P->g.fb == PF_FIELD_R2C) return matvec_r2c<T, S>(P, op, in, out);
+  return matvec_dft<T, S>(P, op, in, out);
+}
+
+// CG helpers use FP64 vectors with FP64 or FP32 transforms
+static pf_status cg_matvec(pf_plan* P, int op, bool fp32, const double* in, double* out) {
+  if (fp32) return matvec_dev<float, double>(P, op, in, out);
+  return matvec_dev<double, double>(P, op, in, out);
+}
+
+#include "pf_cg_host.inc"
+
+static pf_status stage_noise(pf_plan* P, const double* noise, int noise_mem, const double** dev) {
+  *dev = nullptr;
+  if (!noise) return PF_OK;
+  if (noise_mem == PF_MEM_DEVICE) {
+    *dev = noise;
+    return PF_OK;
+  }
+  TRY(ensure(P, (void**)&P->noise_dev, &P->noise_cap, P->g.noise * 8));
+  CK(cudaMemcpyAsync(P->noise_dev, noise, P->g.noise * 8, cudaMemcpyHostToDevice, P->stream));
+  *dev = P->noise_dev;
+  return PF_OK;
+}
+
+template <typename S>
+static pf_status generate_typed(pf_plan* P, const double* nd, uint64_t seed, S* out_dev, int transform) {
+  const bool f64 = sizeof(S) == 8;
+  if (P->g.fb == PF_FIELD_R2C)
+    return f64 ? gen_r2c<double, S>(P, nd, seed, out_dev, transform) : gen_r2c<float, S>(P, nd, seed, out_dev, transform);
+  TRY(ensure(P, &P->spare, &P->spare_cap, P->g.domain * sizeof(S)));
+  TRY(f64 ? gen_dft<double, S>(P, nd, seed, out_dev, (S*)P->spare, transform)
+          : gen_dft<float, S>(P, nd, seed, out_dev, (S*)P->spare, transform));
+  P->spare_valid = true;
+  return PF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void pf_field_desc_init(pf_field_desc* d) {
+  if (!d) return;
+  memset(d, 0, sizeof(*d));
+  d->dim = 2;
+  for (int i = 0; i < 3; i++) {
+    d->cells[i] = 1;
+    d->extensions[i] = 1.0;
+  }
+  d->embedding_factor = 2;
+  d->covariance = PF_COV_EXPONENTIAL;
+  d->variance = 1.0;
+  d->anisotropy = PF_ANISO_NONE;
+  d->corr_length[0] = 1.0;
+  d->matern_nu = 0.5;
+  d->exp_gamma = 1.0;
+  d->cauchy_alpha = 1.0;
+  d->cauchy_beta = 1.0;
+  d->threshold = 1e-14;
+  d->transposed = -1;
+  d->matrix_backend = PF_MATRIX_DEFAULT;
+  d->field_backend = PF_FIELD_DEFAULT;
+  d->precision = PF_PREC_F64;
+  d->eigen_check = PF_EIGCHECK_CORRECTED;
+  d->cg_iterations = 100;
+  d->transform = PF_TRANSFORM_NONE;
+}
+
+pf_status pf_plan_create(const pf_field_desc* desc, pf_plan** plan) {
+  if (!desc || !plan) return fail(PF_ERR_ARG, "null argument");
+  *plan = nullptr;
+  Geom g;
+  TRY(resolve(desc, &g));
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(PF_ERR_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+  }
+  pf_plan* P = new pf_plan();
+  P->desc = *desc;
+  P->g = g;
+  cudaGetDevice(&P->device);
+  e = cudaStreamCreateWithFlags(&P->own, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete P;
+    return fail(PF_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+  }
+  P->stream = P->own;
+  *plan = P;
+  return PF_OK;
+}
+
+void pf_plan_destroy(pf_plan* P) {
+  if (!P) return;
+  cudaStreamSynchronize(P->stream);
+  void** bufs[] = {(void**)&P->lam64, (void**)&P->sq64, (void**)&P->sq32, (void**)&P->lam32, (void**)&P->scan,
+                   &P->ws[0], &P->ws[1], &P->ws[2], (void**)&P->noise_dev, &P->io_dev, &P->io2_dev, &P->spare};
+  for (void** b : bufs)
+    if (*b) cudaFree(*b), *b = nullptr;
+  for (int a = 0; a < 2; a++)
+    for (int o = 0; o < 3; o++)
+      if (P->fac[a][o]) cudaFree(P->fac[a][o]);
+  for (auto& kv : P->tw) cudaFree(kv.second);
+  cg_free(P);
+  for (auto& r : P->recs) {
+    cudaEventDestroy(r.e0);
+    cudaEventDestroy(r.e1);
+  }
+  for (auto e : P->evpool) cudaEventDestroy(e);
+  if (P->own) cudaStreamDestroy(P->own);
+  delete P;
+}
+
+pf_status pf_plan_set_stream(pf_plan* P, void* stream) {
+  if (!P) return fail(PF_ERR_ARG, "null plan");
+  P->stream = stream ? (cudaStream_t)stream : P->own;
+  return PF_OK;
+}
+
+pf_status pf_plan_get_info(const pf_plan* P, pf_plan_info* info) {
+  if (!P || !info) return fail(PF_ERR_ARG, "null argument");
+  memset(info, 0, sizeof(*info));
+  const Geom& g = P->g;
+  info->dim = g.dim;
+  for (int i = 0; i < 3; i++) {
+    info->cells[i] = g.n[i];
+    info->ext_cells[i] = g.T[i];
+  }
+  info->matrix_backend = g.mb;
+  info->field_backend = g.fb;
+  info->transposed = g.transposed;
+  info->precision = P->desc.precision;
+  info->domain_size = g.domain;
+  info->ext_size = g.N;
+  info->spectrum_size = g.S;
+  info->noise_size = g.noise;
+  info->device_bytes = P->bytes_held;
+  return PF_OK;
+}
+
+pf_status pf_spectrum_build(pf_plan* P, pf_eig_stats* stats) {
+  if (!P) return fail(PF_ERR_ARG, "null plan");
+  P->spare_valid = false;
+  pf_status st = build_spectrum(P);
+  if (stats) *stats = P->stats;
+  return check_bounds(P, st);
+}
+
+pf_status pf_spectrum_copy(pf_plan* P, double* out, uint64_t count) {
+  if (!P || !out) return fail(PF_ERR_ARG, "null argument");
+  if (!P->have_spec) return fail(PF_ERR_STATE, "spectrum not built");
+  const Geom& g = P->g;
+  if (count != g.S) return fail(PF_ERR_ARG, "spectrum has %llu entries", (unsigned long long)g.S);
+  std::vector<double> nat(g.S);
+  CK(cudaMemcpyAsync(nat.data(), P->lam64, g.S * 8, cudaMemcpyDeviceToHost, P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  // natural -> the reference's storage order (swap the last two dims when transposed)
+  const int c0 = g.C[0], c1 = g.C[1], c2 = g.C[2];
+  if (!g.transposed) {
+    memcpy(out, nat.data(), g.S * 8);
+  } else if (g.dim == 3) {
+    for (int k2 = 0; k2 < c2; k2++)
+      for (int k1 = 0; k1 < c1; k1++)
+        for (int k0 = 0; k0 < c0; k0++)
+          out[(size_t)k0 + (size_t)c0 * ((size_t)k2 + (size_t)c2 * k1)] =
+              nat[(size_t)k0 + (size_t)c0 * ((size_t)k1 + (size_t)c1 * k2)];
+  } else {
+    for (int k1 = 0; k1 < c1; k1++)
+      for (int k0 = 0; k0 < c0; k0++) out[(size_t)k1 + (size_t)c1 * k0] = nat[(size_t)k0 + (size_t)c0 * k1];
+  }
+  return PF_OK;
+}
+
+pf_status pf_generate(pf_plan* P, const double* noise, int32_t noise_mem, uint64_t seed, void* out, int32_t out_mem,
+                      int32_t apply_transform) {
+  if (!P || !out) return fail(PF_ERR_ARG, "null argument");
+  TRY(ensure_spectrum(P));
+  const size_t es = P->desc.precision == PF_PREC_F64 ? 8 : 4;
+  const size_t bytes = P->g.domain * es;
+  void* dst = out;
+  if (out_mem != PF_MEM_DEVICE) {
+    TRY(ensure(P, &P->io_dev, &P->io_cap, bytes));
+    dst = P->io_dev;
+  }
+  if (P->spare_valid) {  // matrix.hh:416-419: hand out the cached second field
+    CK(cudaMemcpyAsync(dst, P->spare, bytes, cudaMemcpyDeviceToDevice, P->stream));
+    P->spare_valid = false;
+  } else {
+    const double* nd = nullptr;
+    TRY(stage_noise(P, noise, noise_mem, &nd));
+    const int tr = apply_transform ? P->desc.transform : 0;
+    if (es == 8)
+      TRY(generate_typed<double>(P, nd, seed, (double*)dst, tr));
+    else
+      TRY(generate_typed<float>(P, nd, seed, (float*)dst, tr));
+  }
+  if (out_mem != PF_MEM_DEVICE) CK(cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, P->stream));
+  return check_bounds(P, PF_OK);
+}
+
+pf_status pf_generate_batch(pf_plan* P, uint64_t seed, int32_t count, void* out, int32_t out_mem,
+                            int32_t apply_transform) {
+  if (!P || !out || count < 0) return fail(PF_ERR_ARG, "bad argument");
+  TRY(ensure_spectrum(P));
+  const size_t es = P->desc.precision == PF_PREC_F64 ? 8 : 4;
+  const size_t bytes = P->g.domain * es;
+  const int tr = apply_transform ? P->desc.transform : 0;
+  for (int32_t r = 0; r < count; r++) {
+    void* dst = (char*)out + (size_t)r * bytes;
+    if (out_mem != PF_MEM_DEVICE) {
+      TRY(ensure(P, &P->io_dev, &P->io_cap, bytes));
+      dst = P->io_dev;
+    }
+    if (es == 8) {
+      if (P->g.fb == PF_FIELD_R2C)
+        TRY((gen_r2c<double, double>(P, nullptr, seed + r, (double*)dst, tr)));
+      else
+        TRY((generate_typed<double>(P, nullptr, seed + r, (double*)dst, tr)));
+    } else {
+      if (P->g.fb == PF_FIELD_R2C)
+        TRY((gen_r2c<float, float>(P, nullptr, seed + r, (float*)dst, tr)));
+      else
+        TRY((generate_typed<float>(P, nullptr, seed + r, (float*)dst, tr)));
+    }
+    P->spare_valid = false;
+    if (out_mem != PF_MEM_DEVICE)
+      CK(cudaMemcpyAsync((char*)out + (size_t)r * bytes, dst, bytes, cudaMemcpyDeviceToHost, P->stream));
+  }
+  return check_bounds(P, PF_OK);
+}
+
+pf_status pf_matvec(pf_plan* P, int32_t op, int32_t precision, const void* in, void* out, int32_t mem) {
+  if (!P || !in || !out) return fail(PF_ERR_ARG, "null argument");
+  if (op < 0 || op > 2) return fail(PF_ERR_ARG, "unknown operation");
+  TRY(ensure_spectrum(P));
+  const size_t es = precision == PF_PREC_F64 ? 8 : 4;
+  const size_t bytes = P->g.domain * es;
+  const void* src = in;
+  void* dst = out;
+  if (mem != PF_MEM_DEVICE) {
+    TRY(ensure(P, &P->io_dev, &P->io_cap, bytes));
+    TRY(ensure(P, &P->io2_dev, &P->io2_cap, bytes));
+    CK(cudaMemcpyAsync(P->io_dev, in, bytes, cudaMemcpyHostToDevice, P->stream));
+    src = P->io_dev;
+    dst = P->io2_dev;
+  }
+  if (precision == PF_PREC_F64)
+    TRY((matvec_dev<double, double>(P, op, (const double*)src, (double*)dst)));
+  else
+    TRY((matvec_dev<float, float>(P, op, (const float*)src, (float*)dst)));
+  if (mem != PF_MEM_DEVICE) CK(cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, P->stream));
+  return check_bounds(P, PF_OK);
+}
+
+pf_status pf_multiply_inverse(pf_plan* P, const double* b, double* x, int32_t mem, const pf_cg_opts* opts,
+                              pf_cg_report* report) {
+  if (!P || !b || !x) return fail(PF_ERR_ARG, "null argument");
+  TRY(ensure_spectrum(P));
+  pf_cg_opts o;
+  if (opts)
+    o = *opts;
+  else {
+    memset(&o, 0, sizeof(o));
+    o.mode = PF_CG_REFERENCE;
+    o.precondition = 1;
+  }
+  const size_t bytes = P->g.domain * 8;
+  const double* bd = b;
+  double* xd = x;
+  if (mem != PF_MEM_DEVICE) {
+    TRY(ensure(P, &P->io_dev, &P->io_cap, bytes));
+    TRY(ensure(P, &P->io2_dev, &P->io2_cap, bytes));
+    CK(cudaMemcpyAsync(P->io_dev, b, bytes, cudaMemcpyHostToDevice, P->stream));
+    bd = (const double*)P->io_dev;
+    xd = (double*)P->io2_dev;
+  }
+  pf_cg_report rep{};
+  pf_status st = cg_solve(P, bd, xd, o, &rep);
+  if (report) *report = rep;
+  if (st != PF_OK && st != PF_ERR_NOT_CONVERGED) return check_bounds(P, st);
+  if (mem != PF_MEM_DEVICE) CK(cudaMemcpyAsync(x, xd, bytes, cudaMemcpyDeviceToHost, P->stream));
+  return check_bounds(P, st);
+}
+
+pf_status pf_apply_transform(pf_plan* P, int32_t precision, void* data, uint64_t count, int32_t mem) {
+  if (!P || !data) return fail(PF_ERR_ARG, "null argument");
+  const size_t es = precision == PF_PREC_F64 ? 8 : 4;
+  void* d = data;
+  if (mem != PF_MEM_DEVICE) {
+    TRY(ensure(P, &P->io_dev, &P->io_cap, count * es));
+    CK(cudaMemcpyAsync(P->io_dev, data, count * es, cudaMemcpyHostToDevice, P->stream));
+    d = P->io_dev;
+  }
+  ProfRec rec;
+  TRY(prof_begin(P, "transform", count * 2.0 * es, &rec));
+  if (es == 8)
+    k_transform<double><<<grid_for(count), kThreads, 0, P->stream>>>((double*)d, count, P->desc.transform,
+                                                                    P->desc.boxcox_lambda);
+  else
+    k_transform<float><<<grid_for(count), kThreads, 0, P->stream>>>((float*)d, count, P->desc.transform,
+                                                                   P->desc.boxcox_lambda);
+  TRY(prof_end(P, &rec));
+  if (mem != PF_MEM_DEVICE) CK(cudaMemcpyAsync(data, d, count * es, cudaMemcpyDeviceToHost, P->stream));
+  return check_bounds(P, PF_OK);
+}
+
+pf_status pf_profile_enable(pf_plan* P, int32_t enable) {
+  if (!P) return fail(PF_ERR_ARG, "null plan");
+  CK(cudaStreamSynchronize(P->stream));
+  for (auto& r : P->recs) {
+    P->evpool.push_back(r.e0);
+    P->evpool.push_back(r.e1);
+  }
+  P->recs.clear();
+  P->prof = enable != 0;
+  return PF_OK;
+}
+
+pf_status pf_profile_read(pf_plan* P, pf_kernel_time* out, int32_t cap, int32_t* count) {
+  if (!P || !count) return fail(PF_ERR_ARG, "null argument");
+  CK(cudaStreamSynchronize(P->stream));
+  std::vector<std::string> order;
+  std::map<std::string, pf_kernel_time> agg;
+  for (auto& r : P->recs) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, r.e0, r.e1));
+    auto it = agg.find(r.name);
+    if (it == agg.end()) {
+      pf_kernel_time k{};
+      snprintf(k.name, sizeof(k.name), "%s", r.name);
+      it = agg.emplace(r.name, k).first;
+      order.push_back(r.name);
+    }
+    it->second.launches++;
+    it->second.total_ms += ms;
+    it->second.bytes += r.bytes;
+  }
+  int n = 0;
+  for (auto& nm : order) {
+    if (n < cap && out) out[n] = agg[nm];
+    n++;
+  }
+  *count = n;
+  return PF_OK;
+}
+
+uint64_t pf_launch_count(const pf_plan* P) { return P ? P->launches : 0; }
+
+const char* pf_last_error_string(void) { return g_err.c_str(); }
+
+const char* pf_version(void) { return "parafields-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,758 @@
+// pf_kernels.cuh -- pass kernels and the functors fused into their load/store stages.
+#pragma once
+
+#include <math.h>
+
+#include "pf_fft.cuh"
+
+namespace pf {
+
+constexpr int kThreads = 256;
+
+// Set by any functor whose computed index falls outside its buffer; the access is
+// skipped instead of performed, and the host turns the flag into an error.
+__device__ unsigned int g_bounds_error;
+
+__device__ __forceinline__ bool in_bounds(long long i, long long n) {
+  if (i >= 0 && i < n) return true;
+  atomicOr(&g_bounds_error, 1u);
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// pass descriptor
+// ---------------------------------------------------------------------------
+struct PassArgs {
+  int L;               // complex transform length
+  int Lout;            // outputs stored per pencil (pruning)
+  int B;               // pencils per tile
+  int pitch;           // shared-memory pitch of one pencil (contiguous passes)
+  long long npencil;   // contiguous: rows; strided: inner extent
+  long long nouter;    // strided: outer extent
+  int sign, sign2;     // first / second (fused) transform direction
+  Radices rad;         // radix schedule of L
+};
+
+struct NoMid {
+  static constexpr bool active = false;
+  template <typename T>
+  __device__ cx<T> operator()(long long, int, long long, cx<T> v) const {
+    return v;
+  }
+};
+
+// Generic complex pencil pass.  CONTIG: pencils are rows (element j of row p at
+// stride 1); otherwise pencil p of outer block o has element j at p + j*jstride +
+// o*ostride, and one tile holds B consecutive p so every row segment is coalesced.
+template <typename T, bool CONTIG, class Ld, class Mid, class St>
+__global__ void __launch_bounds__(kThreads) k_pass(const PassArgs a, const cx<T>* __restrict__ tw,
+                                                   Ld ld, Mid mid, St st) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
+  TileShape ts;
+  ts.L = a.L;
+  ts.B = a.B;
+  if (CONTIG) {
+    ts.sb = a.pitch;
+    ts.sj = 1;
+    ts.bfast = 0;
+  } else {
+    ts.sb = 1;
+    ts.sj = a.B;
+    ts.bfast = 1;
+  }
+  cx<T>* b1 = b0 + (CONTIG ? a.B * a.pitch : a.B * a.L);
+  long long p0, io;
+  if (CONTIG) {
+    p0 = (long long)blockIdx.x * a.B;
+    io = 0;
+  } else {
+    const long long tpo = (a.npencil + a.B - 1) / a.B;
+    io = blockIdx.x / tpo;
+    p0 = (blockIdx.x - io * tpo) * a.B;
+  }
+  const int tot = a.B * a.L;
+  for (int u = threadIdx.x; u < tot; u += blockDim.x) {
+    int b, j;
+    if (CONTIG) {
+      b = u / a.L;
+      j = u - b * a.L;
+    } else {
+      b = u % a.B;
+      j = u / a.B;
+    }
+    const long long p = p0 + b;
+    b0[b * ts.sb + j * ts.sj] = (p < a.npencil) ? ld.template load<T>(p, j, io) : mk<T>(0, 0);
+  }
+  __syncthreads();
+  cx<T>* r = fft_tile<T>(b0, b1, ts, a.rad, tw, a.sign);
+  if (Mid::active) {
+    for (int u = threadIdx.x; u < tot; u += blockDim.x) {
+      int b, j;
+      if (CONTIG) {
+        b = u / a.L;
+        j = u - b * a.L;
+      } else {
+        b = u % a.B;
+        j = u / a.B;
+      }
+      const long long p = p0 + b;
+      if (p < a.npencil) r[b * ts.sb + j * ts.sj] = mid.template operator()<T>(p, j, io, r[b * ts.sb + j * ts.sj]);
+    }
+    __syncthreads();
+    r = fft_tile<T>(r, r == b0 ? b1 : b0, ts, a.rad, tw, a.sign2);
+  }
+  const int tout = a.B * a.Lout;
+  for (int u = threadIdx.x; u < tout; u += blockDim.x) {
+    int b, j;
+    if (CONTIG) {
+      b = u / a.Lout;
+      j = u - b * a.Lout;
+    } else {
+      b = u % a.B;
+      j = u / a.B;
+    }
+    const long long p = p0 + b;
+    if (p < a.npencil) st.template store<T>(p, j, io, r[b * ts.sb + j * ts.sj]);
+  }
+}
+
+// Real-to-complex pass along dimension 0 (rows of 2L reals -> L+1 complex), via the
+// half-length complex FFT of z_m = x_{2m} + i x_{2m+1} and the standard split
+// X_k = (Z_k + conj Z_{L-k})/2 - i/2 e^{-2 pi i k/2L} (Z_k - conj Z_{L-k}).
+// twT holds exp(-2 pi i m / 2L).
+template <typename T, class Ld, class St>
+__global__ void __launch_bounds__(kThreads) k_r2c(const PassArgs a, const cx<T>* __restrict__ tw,
+                                                  const cx<T>* __restrict__ twT, Ld ld, St st) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
+  cx<T>* b1 = b0 + a.B * a.pitch;
+  TileShape ts{a.L, a.B, a.pitch, 1, 0};
+  const long long p0 = (long long)blockIdx.x * a.B;
+  const int tot = a.B * a.L;
+  for (int u = threadIdx.x; u < tot; u += blockDim.x) {
+    const int b = u / a.L, m = u - b * a.L;
+    const long long p = p0 + b;
+    cx<T> z = mk<T>(0, 0);
+    if (p < a.npencil) z = mk<T>(ld.template real<T>(p, 2 * m), ld.template real<T>(p, 2 * m + 1));
+    b0[b * a.pitch + m] = z;
+  }
+  __syncthreads();
+  cx<T>* Z = fft_tile<T>(b0, b1, ts, a.rad, tw, -1);
+  cx<T>* X = (Z == b0) ? b1 : b0;
+  const int L = a.L;
+  for (int u = threadIdx.x; u < a.B * (L + 1); u += blockDim.x) {
+    const int b = u / (L + 1), k = u - b * (L + 1);
+    const cx<T> zk = Z[b * a.pitch + (k == L ? 0 : k)];
+    const cx<T> zm = conjg<T>(Z[b * a.pitch + (k == 0 ? 0 : L - k)]);
+    const cx<T> e = cscale<T>(cadd<T>(zk, zm), (T)0.5);
+    const cx<T> o = cscale<T>(csub<T>(zk, zm), (T)0.5);  // (Zk - conj Z_{L-k})/2
+    // o / i = -i o ; times w = exp(-2 pi i k / 2L)
+    const cx<T> oi = mk<T>(o.y, -o.x);
+    const cx<T> w = (k == L) ? mk<T>(-1, 0) : __ldg(twT + k);
+    X[b * a.pitch + k] = cadd<T>(e, cmul<T>(oi, w));
+  }
+  __syncthreads();
+  for (int u = threadIdx.x; u < a.B * a.Lout; u += blockDim.x) {
+    const int b = u / a.Lout, k = u - b * a.Lout;
+    const long long p = p0 + b;
+    if (p < a.npencil) st.template store<T>(p, k, 0, X[b * a.pitch + k]);
+  }
+}
+
+// Complex-to-real pass along dimension 0 with FFTW c2r semantics (imaginary parts of
+// the DC and Nyquist entries ignored): Z_k = (X_k + conj X_{L-k}) + i e^{+2 pi i k/2L}
+// (X_k - conj X_{L-k}), z = IDFT_L(Z), out_{2m} = Re z_m, out_{2m+1} = Im z_m.
+template <typename T, class Ld, class St>
+__global__ void __launch_bounds__(kThreads) k_c2r(const PassArgs a, const cx<T>* __restrict__ tw,
+                                                  const cx<T>* __restrict__ twT, Ld ld, St st) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
+  cx<T>* b1 = b0 + a.B * a.pitch;
+  TileShape ts{a.L, a.B, a.pitch, 1, 0};
+  const long long p0 = (long long)blockIdx.x * a.B;
+  const int L = a.L;
+  for (int u = threadIdx.x; u < a.B * (L + 1); u += blockDim.x) {
+    const int b = u / (L + 1), k = u - b * (L + 1);
+    const long long p = p0 + b;
+    cx<T> v = (p < a.npencil) ? ld.template load<T>(p, k, 0) : mk<T>(0, 0);
+    if (k == 0 || k == L) v.y = 0;
+    b1[b * a.pitch + k] = v;
+  }
+  __syncthreads();
+  for (int u = threadIdx.x; u < a.B * L; u += blockDim.x) {
+    const int b = u / L, k = u - b * L;
+    const cx<T> xk = b1[b * a.pitch + k];
+    const cx<T> xm = conjg<T>(b1[b * a.pitch + L - k]);
+    const cx<T> s = cadd<T>(xk, xm);
+    const cx<T> d = csub<T>(xk, xm);
+    const cx<T> w = conjg<T>(__ldg(twT + k));  // exp(+2 pi i k / 2L)
+    const cx<T> t = cmul<T>(d, w);
+    b0[b * a.pitch + k] = mk<T>(s.x - t.y, s.y + t.x);  // s + i t
+  }
+  __syncthreads();
+  cx<T>* z = fft_tile<T>(b0, b1, ts, a.rad, tw, +1);
+  for (int u = threadIdx.x; u < a.B * a.Lout; u += blockDim.x) {
+    const int b = u / a.Lout, j = u - b * a.Lout;
+    const long long p = p0 + b;
+    if (p < a.npencil) {
+      const cx<T> v = z[b * a.pitch + (j >> 1)];
+      st.template real<T>(p, j, (j & 1) ? v.y : v.x);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// array load/store functors (element p + j*jstride + o*ostride, complex)
+// ---------------------------------------------------------------------------
+template <typename S>
+struct ArrLoad {
+  const S* ptr;  // S = float2 or double2
+  long long jstride, ostride, rowstride;
+  long long n;  // elements in the buffer
+  int Lin;      // j >= Lin reads zero (input pruning / zero padding)
+  template <typename T>
+  __device__ __forceinline__ cx<T> load(long long p, int j, long long o) const {
+    if (j >= Lin) return mk<T>(0, 0);
+    const long long i = p * rowstride + j * jstride + o * ostride;
+    if (!in_bounds(i, n)) return mk<T>(0, 0);
+    const S v = ptr[i];
+    return mk<T>((T)v.x, (T)v.y);
+  }
+};
+
+template <typename S>
+struct ArrStore {
+  S* ptr;
+  long long jstride, ostride, rowstride;
+  long long n;
+  template <typename T>
+  __device__ __forceinline__ void store(long long p, int j, long long o, cx<T> v) const {
+    const long long i = p * rowstride + j * jstride + o * ostride;
+    if (!in_bounds(i, n)) return;
+    S w;
+    w.x = v.x;
+    w.y = v.y;
+    ptr[i] = w;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// value transforms (mutators.hh:35-118)
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T apply_mutator(int kind, T lam, T v) {
+  switch (kind) {
+    case 1: return exp(v);
+    case 2: return fabs(v);
+    case 3: return v < (T)0 ? (T)-1 : (T)1;
+    case 4: return pow(v * lam + (T)1, -lam);
+    default: return v;
+  }
+}
+
+// real row load of a field embedded in the torus (fieldToExtendedField,
+// r2cfieldbackend.hh:352-368): row p holds x[p*n0 + j] for j < n0, zero beyond
+template <typename S>
+struct FieldRowLoad {
+  const S* x;
+  int n0;
+  long long n;
+  template <typename T>
+  __device__ __forceinline__ T real(long long p, int j) const {
+    if (j >= n0) return (T)0;
+    const long long i = p * n0 + j;
+    return in_bounds(i, n) ? (T)x[i] : (T)0;
+  }
+};
+
+// real row store of the original-domain corner (extendedFieldToField,
+// r2cfieldbackend.hh:433-441) with an optional value transform
+template <typename S>
+struct FieldRowStore {
+  S* out;
+  int n0;
+  int transform;
+  double boxcox;
+  long long n;
+  template <typename T>
+  __device__ __forceinline__ void real(long long p, int j, T v) const {
+    if (transform) v = apply_mutator<T>(transform, (T)boxcox, v);
+    const long long i = p * n0 + j;
+    if (in_bounds(i, n)) out[i] = (S)v;
+  }
+};
+
+// complex row store splitting Re / Im into two fields (DFT backend, component 0/1,
+// dftfieldbackend.hh:380-393)
+template <typename S>
+struct SplitStore {
+  S* re;
+  S* im;  // may be null
+  long long rowlen;
+  int transform;
+  double boxcox;
+  long long n;
+  template <typename T>
+  __device__ __forceinline__ void store(long long p, int j, long long, cx<T> v) const {
+    T a = v.x, b = v.y;
+    if (transform) {
+      a = apply_mutator<T>(transform, (T)boxcox, a);
+      b = apply_mutator<T>(transform, (T)boxcox, b);
+    }
+    const long long i = p * rowlen + j;
+    if (!in_bounds(i, n)) return;
+    re[i] = (S)a;
+    if (im) im[i] = (S)b;
+  }
+};
+
+// complex row load of a real field (DFT backend embedding, dftfieldbackend.hh:307-325)
+template <typename S>
+struct FieldComplexLoad {
+  const S* x;
+  int n0;
+  long long n;
+  template <typename T>
+  __device__ __forceinline__ cx<T> load(long long p, int j, long long) const {
+    if (j >= n0) return mk<T>(0, 0);
+    const long long i = p * n0 + j;
+    return mk<T>(in_bounds(i, n) ? (T)x[i] : (T)0, (T)0);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// covariance evaluation on the torus (matrix.hh:615-638, covariance.hh)
+// ---------------------------------------------------------------------------
+struct CovParams {
+  int dim;
+  int cov;
+  int aniso;
+  int T[3];
+  int rowcells[3];  // cells of the row decomposition (dim 0 is the pencil)
+  double h[3];
+  double half[3];   // 0.5 * ext * factor
+  double wrap[3];   // ext * factor
+  double geo[9];    // transformation applied to coordinates
+  double variance;
+  double p0, p1;    // gamma / alpha / beta
+};
+
+__device__ __forceinline__ double cov_eval(const CovParams& c, const double* xt) {
+  const double var = c.variance;
+  const int dim = c.dim;
+  double sum = 0.;
+  for (int i = 0; i < dim; i++) sum += xt[i] * xt[i];
+  switch (c.cov) {
+    case 2: {  // spherical, covariance.hh:310-340
+      const double h = sqrt(sum);
+      if (h > 1.) return 0.;
+      if (dim == 3) return var * (1. - 1.5 * h + 0.5 * pow(h, 3.));
+      if (dim == 2)
+        return var * (1. - 2. / 3.14159265358979323846 * (h * sqrt(1. - pow(h, 2.)) + asin(h)));
+      return var * (1. - h);
+    }
+    case 0: return var * exp(-sqrt(sum));                   // exponential
+    case 8: return var * exp(-pow(sqrt(sum), c.p0));        // gammaExponential
+    case 1: {                                               // gaussian
+      const double h = sqrt(sum);
+      return var * exp(-h * h);
+    }
+    case 3: {  // separableExponential
+      double s = 0.;
+      for (int i = 0; i < dim; i++) s += fabs(xt[i]);
+      return var * exp(-s);
+    }
+    case 5: {  // matern32
+      const double h = sqrt(sum);
+      return var * (1. + sqrt(3.) * h) * exp(-sqrt(3.) * h);
+    }
+    case 6: {  // matern52
+      const double h = sqrt(sum);
+      return var * (1. + sqrt(5.) * h + 5. / 3. * h * h) * exp(-sqrt(5.) * h);
+    }
+    case 7: {  // dampedOscillation
+      const double h = sqrt(sum);
+      if (dim == 3) return var * exp(-h) * cos(h / sqrt(3.));
+      return var * exp(-h) * cos(h);
+    }
+    case 9: {  // cauchy
+      const double h = sqrt(sum);
+      return var * pow(1. + pow(h, 2.), -3.);
+    }
+    case 10: {  // generalizedCauchy
+      const double h = sqrt(sum);
+      return var * pow(1. + pow(h, c.p0), -c.p1);
+    }
+    case 11: {  // cubic
+      const double h = sqrt(sum);
+      if (h > 1.) return 0.;
+      return var * (1. - 7. * pow(h, 2.) + 8.75 * pow(h, 3.) - 3.5 * pow(h, 5.) + 0.75 * pow(h, 7.));
+    }
+    case 12:  // whiteNoise
+      for (int i = 0; i < dim; i++)
+        if (fabs(xt[i]) > 1e-10) return 0.;
+      return var;
+    default: return 0.;
+  }
+}
+
+// covariance at torus cell (j0, j1, j2) with the classical mirroring
+__device__ __forceinline__ double cov_at(const CovParams& c, int j0, int j1, int j2) {
+  const int jj[3] = {j0, j1, j2};
+  double x[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
+  for (int i = 0; i < c.dim; i++) {
+    double v = (double)(unsigned int)jj[i] * c.h[i];
+    if (v > c.half[i]) v -= c.wrap[i];
+    x[i] = v;
+  }
+  if (c.aniso == 0) {
+    for (int i = 0; i < c.dim; i++) xt[i] = c.geo[0] * x[i];
+  } else if (c.aniso == 1) {
+    for (int i = 0; i < c.dim; i++) xt[i] = c.geo[i] * x[i];
+  } else {
+    for (int i = 0; i < c.dim; i++) {
+      double s = 0.;
+      for (int k = 0; k < c.dim; k++) s += c.geo[i * c.dim + k] * x[k];
+      xt[i] = s;
+    }
+  }
+  return cov_eval(c, xt);
+}
+
+// row p of the torus (dims 1..d-1 flattened), element j along dim 0
+struct CovRowLoad {
+  CovParams c;
+  template <typename T>
+  __device__ __forceinline__ T real(long long p, int j) const {
+    const int j1 = c.dim > 1 ? (int)(p % c.T[1]) : 0;
+    const int j2 = c.dim > 2 ? (int)(p / c.T[1]) : 0;
+    return (T)cov_at(c, j, j1, j2);
+  }
+  template <typename T>
+  __device__ __forceinline__ cx<T> load(long long p, int j, long long) const {
+    return mk<T>(real<T>(p, j), (T)0);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// counter-based normal noise: Philox2x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel
+// random numbers: as easy as 1, 2, 3", SC 2011) + Box-Muller
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint2 philox2x32_10(uint2 ctr, uint32_t key) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    const uint32_t lo = ctr.x * 0xD256D193u;
+    const uint32_t hi = __umulhi(ctr.x, 0xD256D193u);
+    ctr = make_uint2(hi ^ key ^ ctr.y, lo);
+    key += 0x9E3779B9u;
+  }
+  return ctr;
+}
+
+__device__ __forceinline__ void sincospi_any(float x, float* s, float* c) { sincospif(x, s, c); }
+__device__ __forceinline__ void sincospi_any(double x, double* s, double* c) { sincospi(x, s, c); }
+
+template <typename T>
+__device__ __forceinline__ void normal_pair(uint64_t seed, uint64_t idx, T& r1, T& r2) {
+  const uint2 c = philox2x32_10(make_uint2((uint32_t)idx, (uint32_t)(idx >> 32) ^ (uint32_t)(seed >> 32)),
+                                (uint32_t)seed);
+  // u1 in (0, 1], u2 in [0, 1)
+  const T u1 = ((T)(c.x >> 8) + (T)1) * (T)(1.0 / 16777216.0);
+  const T u2 = (T)(c.y >> 8) * (T)(1.0 / 16777216.0);
+  const T rad = sqrt((T)-2 * log(u1));
+  T s, co;
+  sincospi_any(2 * u2, &s, &co);
+  r1 = rad * co;
+  r2 = rad * s;
+}
+
+// ---------------------------------------------------------------------------
+// noise x sqrt(eigenvalue) in the R2C half spectrum (R2CFieldBackend::set,
+// r2cfieldbackend.hh:305-325 fed by generateField, matrix.hh:375-404)
+// ---------------------------------------------------------------------------
+struct R2CNoise {
+  int dim;
+  int ext[3];
+  int T0c;
+  int transposed;
+  int dct;            // eigenvalue layout: 1 = DCT prod(T/2+1), 0 = half spectrum, 2 = full spectrum
+  int D0, D1;         // DCT cells of dims 0 and 1
+  const void* sq;     // sqrt(lambda), float or double per the pass precision
+  const double* noise;  // reference draw order, or null for the counter-based generator
+  uint64_t seed;
+  long long nsq, nnoise;  // buffer sizes (eigenvalues, noise doubles)
+  // pass geometry: the transform axis is dim-1 (first backward pass)
+  template <typename T>
+  __device__ __forceinline__ cx<T> load(long long p, int j, long long) const {
+    const int k0 = (int)(p % T0c);
+    const int k1 = dim == 3 ? (int)(p / T0c) : j;
+    const int k2 = dim == 3 ? j : 0;
+    // stored (reference) index of this frequency
+    uint64_t si;
+    if (transposed)
+      si = (uint64_t)k0 + (uint64_t)T0c * ((uint64_t)k2 + (uint64_t)ext[2] * (uint64_t)k1);
+    else
+      si = (uint64_t)k0 + (uint64_t)T0c * ((uint64_t)k1 + (uint64_t)ext[1] * (uint64_t)k2);
+    uint64_t li;
+    if (dct == 1) {
+      const int m1 = k1 <= ext[1] / 2 ? k1 : ext[1] - k1;
+      const int m2 = k2 <= ext[2] / 2 ? k2 : ext[2] - k2;
+      li = (uint64_t)k0 + (uint64_t)D0 * ((uint64_t)m1 + (uint64_t)D1 * (uint64_t)m2);
+    } else if (dct == 2) {  // full DFT spectrum (dftmatrixbackend.hh:303-307)
+      li = (uint64_t)k0 + (uint64_t)ext[0] * ((uint64_t)k1 + (uint64_t)ext[1] * (uint64_t)k2);
+    } else {
+      li = (uint64_t)k0 + (uint64_t)T0c * ((uint64_t)k1 + (uint64_t)ext[1] * (uint64_t)k2);
+    }
+    if (!in_bounds((long long)li, nsq)) return mk<T>(0, 0);
+    const T lam = ((const T*)sq)[li];
+    T r1, r2;
+    if (noise) {
+      if (!in_bounds((long long)(2 * si + 1), nnoise)) return mk<T>(0, 0);
+      r1 = (T)noise[2 * si];
+      r2 = (T)noise[2 * si + 1];
+    } else {
+      normal_pair<T>(seed, si, r1, r2);
+    }
+    const bool selfconj = ((2 * k0) % ext[0] == 0) && ((2 * k1) % ext[1] == 0) && (dim < 3 || (2 * k2) % ext[2] == 0);
+    if (selfconj) return mk<T>(lam * r1, (T)0);
+    const T s = lam / (T)1.41421356237309504880168872420969808;
+    return mk<T>(s * r1, s * r2);
+  }
+};
+
+// full-torus complex noise of the DFT backend (dftfieldbackend.hh:276-280); the pass
+// runs along the slowest dimension d-1 first (contiguous when dim == 1)
+struct DFTNoise {
+  int dim;
+  int ext[3];
+  int Ts[3];
+  int transposed;
+  int mat;  // 0 DCT (mirrored lookup), 2 DFT (full layout, stored order)
+  const void* sq;
+  const double* noise;
+  uint64_t seed;
+  long long nsq, nnoise;
+  template <typename T>
+  __device__ __forceinline__ cx<T> load(long long p, int j, long long) const {
+    int k[3] = {0, 0, 0};
+    if (dim == 1) {
+      k[0] = j;
+    } else if (dim == 2) {
+      k[0] = (int)p;
+      k[1] = j;
+    } else {
+      k[0] = (int)(p % ext[0]);
+      k[1] = (int)(p / ext[0]);
+      k[2] = j;
+    }
+    int a[3] = {k[0], k[1], k[2]};
+    if (transposed) {
+      const int x = dim - 1, y = dim - 2;
+      const int t = a[x];
+      a[x] = a[y];
+      a[y] = t;
+    }
+    const uint64_t si = (uint64_t)a[0] + (uint64_t)Ts[0] * ((uint64_t)a[1] + (uint64_t)Ts[1] * (uint64_t)a[2]);
+    uint64_t li;
+    if (mat == 0) {
+      int m[3];
+      int D[3];
+      for (int i = 0; i < 3; i++) {
+        D[i] = ext[i] / 2 + 1;
+        m[i] = k[i] <= ext[i] / 2 ? k[i] : ext[i] - k[i];
+      }
+      li = (uint64_t)m[0] + (uint64_t)D[0] * ((uint64_t)m[1] + (uint64_t)D[1] * (uint64_t)m[2]);
+    } else {
+      li = (uint64_t)k[0] + (uint64_t)ext[0] * ((uint64_t)k[1] + (uint64_t)ext[1] * (uint64_t)k[2]);
+    }
+    if (!in_bounds((long long)li, nsq)) return mk<T>(0, 0);
+    const T lam = ((const T*)sq)[li];
+    T r1, r2;
+    if (noise) {
+      if (!in_bounds((long long)(2 * si + 1), nnoise)) return mk<T>(0, 0);
+      r1 = (T)noise[2 * si];
+      r2 = (T)noise[2 * si + 1];
+    } else {
+      normal_pair<T>(seed, si, r1, r2);
+    }
+    return mk<T>(lam * r1, lam * r2);
+  }
+};
+
+// eigenvalue factor lookup for the fused matvec pass (fieldBackend.mult,
+// r2cfieldbackend.hh:337-341 with matrixBackend.eval, matrix.hh:1482-1495)
+struct MultMid {
+  static constexpr bool active = true;
+  int dim;
+  int ext[3];
+  int C0;        // cells of dim 0 in the frequency array (T0/2+1 for R2C, T0 for DFT)
+  int LC0;       // cells of dim 0 in the eigenvalue array (layouts 1 and 2)
+  int layout;    // 0 DCT, 1 natural half spectrum, 2 natural full spectrum
+  int D0, D1;
+  int axis;      // axis of the fused pass (dim-1)
+  const void* fac;  // factor per stored eigenvalue (precision of the pass)
+  long long nfac;
+  template <typename T>
+  __device__ __forceinline__ cx<T> operator()(long long p, int j, long long, cx<T> v) const {
+    int k0, k1 = 0, k2 = 0;
+    if (dim == 1) {
+      k0 = j;
+    } else if (dim == 2) {
+      k0 = (int)p;
+      k1 = j;
+    } else {
+      k0 = (int)(p % C0);
+      k1 = (int)(p / C0);
+      k2 = j;
+    }
+    uint64_t li;
+    if (layout == 0) {
+      const int m0 = k0 <= ext[0] / 2 ? k0 : ext[0] - k0;
+      const int m1 = k1 <= ext[1] / 2 ? k1 : ext[1] - k1;
+      const int m2 = k2 <= ext[2] / 2 ? k2 : ext[2] - k2;
+      li = (uint64_t)m0 + (uint64_t)D0 * ((uint64_t)m1 + (uint64_t)D1 * (uint64_t)m2);
+    } else {
+      li = (uint64_t)k0 + (uint64_t)LC0 * ((uint64_t)k1 + (uint64_t)ext[1] * (uint64_t)k2);
+    }
+    if (!in_bounds((long long)li, nfac)) return mk<T>(0, 0);
+    const T f = ((const T*)fac)[li];
+    return mk<T>(v.x * f, v.y * f);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// eigenvalue scan (matrix.hh:266-317) over the transformed spectrum
+// ---------------------------------------------------------------------------
+struct ScanOut {
+  unsigned int small, zero, negative, pad;
+  unsigned long long minkey;
+};
+
+__device__ __forceinline__ unsigned long long dkey(double v) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+struct ScanArgs {
+  const double2* spec;  // complex spectrum, natural layout, cells C[0..2]
+  int C[3];
+  int Ts[3];            // stored layout cells (swapped when transposed)
+  int transposed;
+  int dim;
+  int faithful;         // reference real-view scan (R2C only)
+  uint64_t count;
+  double N;
+  double threshold;
+  double* lam;          // out: eigenvalues, natural layout
+  double* sq64;
+  float* sq32;
+  float* lam32;
+  ScanOut* out;
+};
+
+__device__ __forceinline__ void scan_one(double v, double thr, unsigned int& sm, unsigned int& ze,
+                                         unsigned int& ne, double& mn) {
+  if (v < mn) mn = v;
+  if (v < 1e-6) {
+    if (v < thr) {
+      if (v > -thr)
+        ze++;
+      else
+        ne++;
+    } else
+      sm++;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_scan(const ScanArgs a) {
+  unsigned int sm = 0, ze = 0, ne = 0;
+  double mn = 1.7976931348623157e308;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.count; i += stride) {
+    const double2 z = a.spec[i];
+    double re = z.x / a.N, im = z.y / a.N;
+    if (a.faithful) {
+      // position of this entry in the reference's stored (possibly transposed) order
+      const uint64_t k0 = i % a.C[0];
+      const uint64_t r = i / a.C[0];
+      const uint64_t k1 = r % a.C[1];
+      const uint64_t k2 = r / a.C[1];
+      uint64_t si;
+      if (a.transposed && a.dim == 3)
+        si = k0 + (uint64_t)a.C[0] * (k2 + (uint64_t)a.C[2] * k1);
+      else
+        si = i;
+      if (2 * si < a.count) {
+        scan_one(re, a.threshold, sm, ze, ne, mn);
+        if (re < 0.) re = 0.;
+      }
+      if (2 * si + 1 < a.count) scan_one(im, a.threshold, sm, ze, ne, mn);
+    } else {
+      scan_one(re, a.threshold, sm, ze, ne, mn);
+      if (re < 0.) re = 0.;
+    }
+    a.lam[i] = re;
+    const double s = sqrt(re);
+    a.sq64[i] = s;
+    a.sq32[i] = (float)s;
+    a.lam32[i] = (float)re;
+  }
+  // block reduction
+  __shared__ unsigned int rs[3][kThreads / 32];
+  __shared__ double rm[kThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    sm += __shfl_down_sync(0xffffffffu, sm, o);
+    ze += __shfl_down_sync(0xffffffffu, ze, o);
+    ne += __shfl_down_sync(0xffffffffu, ne, o);
+    mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    rs[0][w] = sm;
+    rs[1][w] = ze;
+    rs[2][w] = ne;
+    rm[w] = mn;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < kThreads / 32; k++) {
+      sm += rs[0][k];
+      ze += rs[1][k];
+      ne += rs[2][k];
+      mn = fmin(mn, rm[k]);
+    }
+    if (sm) atomicAdd(&a.out->small, sm);
+    if (ze) atomicAdd(&a.out->zero, ze);
+    if (ne) atomicAdd(&a.out->negative, ne);
+    atomicMin(&a.out->minkey, dkey(mn));
+  }
+}
+
+// DFT-matrix spectrum scan: get() is the real part and set() clears both parts
+// (dftmatrixbackend.hh:322-338); same statistics as above.
+// (covered by k_scan with faithful = 0 over the full complex torus.)
+
+// factor arrays for the matvecs: lambda/N, sqrt(lambda)/N, 1/(lambda N)
+template <typename T>
+__global__ void k_factors(const double* __restrict__ lam, uint64_t n, double invN, int op, T* out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const double l = lam[i];
+    double f;
+    if (op == 0)
+      f = l * invN;
+    else if (op == 1)
+      f = sqrt(l) * invN;
+    else
+      f = (1. / l) * invN;
+    out[i] = (T)f;
+  }
+}
+
+template <typename S>
+__global__ void k_transform(S* v, uint64_t n, int kind, double lam) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    v[i] = apply_mutator<S>(kind, (S)lam, v[i]);
+}
+
+}  // namespace pf

@@ -1,0 +1,298 @@
+"""ctypes binding of libpfcuda.so, the C ABI in include/parafields_b200.h.
+
+This is the Python-side mirror of the reference's Matrix API for the
+circulant-embedding path (include/parafields/matrix.hh:142-421, 1443-1646) used
+by the tests and the benchmark.  The CUDA library is loaded on first use and the
+binding raises if it is missing: there is no CPU fallback.
+
+Array arguments are numpy arrays (host memory) or torch CUDA tensors (device
+memory, passed by data_ptr()).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libpfcuda.so")
+
+# --- enums (include/parafields_b200.h) ---------------------------------------
+PF_OK, PF_ERR_NEG_EIGEN, PF_ERR_CONFIG, PF_ERR_OOM, PF_ERR_CUDA = 0, 1, 2, 3, 4
+PF_ERR_NOT_CONVERGED, PF_ERR_TIMEOUT, PF_ERR_STATE, PF_ERR_ARG = 5, 6, 7, 8
+
+COVARIANCES = {
+    "exponential": 0, "gaussian": 1, "spherical": 2, "separableExponential": 3,
+    "matern": 4, "matern32": 5, "matern52": 6, "dampedOscillation": 7,
+    "gammaExponential": 8, "cauchy": 9, "generalizedCauchy": 10, "cubic": 11,
+    "whiteNoise": 12,
+}
+ANISOTROPIES = {"none": 0, "axiparallel": 1, "geometric": 2}
+TRANSFORMS = {"none": 0, "logNormal": 1, "foldedNormal": 2, "sign": 3, "boxCox": 4}
+MATRIX_DCT, MATRIX_R2C, MATRIX_DFT = 0, 1, 2
+FIELD_R2C, FIELD_DFT, FIELD_DCTDST = 0, 1, 2
+PREC_F64, PREC_F32 = 0, 1
+EIGCHECK_CORRECTED, EIGCHECK_REFERENCE = 0, 1
+OP_MUL, OP_ROOT, OP_INVEXT = 0, 1, 2
+MEM_HOST, MEM_DEVICE = 0, 1
+CG_REFERENCE, CG_RESIDUAL = 0, 1
+
+
+class FieldDesc(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32), ("cells", C.c_int32 * 3), ("extensions", C.c_double * 3),
+        ("embedding_factor", C.c_int32), ("periodic", C.c_int32), ("covariance", C.c_int32),
+        ("variance", C.c_double), ("anisotropy", C.c_int32), ("corr_length", C.c_double * 9),
+        ("matern_nu", C.c_double), ("exp_gamma", C.c_double), ("cauchy_alpha", C.c_double),
+        ("cauchy_beta", C.c_double), ("approximate", C.c_int32), ("threshold", C.c_double),
+        ("transposed", C.c_int32), ("matrix_backend", C.c_int32), ("field_backend", C.c_int32),
+        ("precision", C.c_int32), ("eigen_check", C.c_int32), ("cg_iterations", C.c_int32),
+        ("transform", C.c_int32), ("boxcox_lambda", C.c_double),
+    ]
+
+
+class EigStats(C.Structure):
+    _fields_ = [("small", C.c_uint32), ("zero", C.c_uint32), ("negative", C.c_uint32),
+                ("pad_", C.c_uint32), ("smallest", C.c_double)]
+
+    def as_dict(self):
+        return {"small": self.small, "zero": self.zero, "negative": self.negative,
+                "smallest": self.smallest}
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32), ("cells", C.c_int32 * 3), ("ext_cells", C.c_int32 * 3),
+        ("matrix_backend", C.c_int32), ("field_backend", C.c_int32), ("transposed", C.c_int32),
+        ("precision", C.c_int32), ("domain_size", C.c_uint64), ("ext_size", C.c_uint64),
+        ("spectrum_size", C.c_uint64), ("noise_size", C.c_uint64), ("device_bytes", C.c_uint64),
+    ]
+
+
+class CgOpts(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("max_iterations", C.c_int32), ("tolerance", C.c_double),
+                ("inner_fp32", C.c_int32), ("precondition", C.c_int32)]
+
+
+class CgReport(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("refinements", C.c_int32),
+                ("relative_residual", C.c_double)]
+
+
+class KernelTime(C.Structure):
+    _fields_ = [("name", C.c_char * 48), ("launches", C.c_uint64), ("total_ms", C.c_double),
+                ("bytes", C.c_double)]
+
+
+def make_desc(dim=2, cells=(16, 16), extensions=None, covariance="exponential", variance=1.0,
+              corr_length=0.05, anisotropy=None, embedding_factor=2, periodic=False,
+              approximate=False, threshold=1e-14, transposed=-1, matrix_backend=-1,
+              field_backend=-1, precision=PREC_F64, eigen_check=EIGCHECK_CORRECTED,
+              cg_iterations=100, transform="none", boxcox_lambda=0.0, matern_nu=0.5,
+              exp_gamma=1.0, cauchy_alpha=1.0, cauchy_beta=1.0) -> FieldDesc:
+    """Builds a descriptor from values named after the reference's config keys."""
+    d = FieldDesc()
+    d.dim = dim
+    for i in range(3):
+        d.cells[i] = int(cells[i]) if i < dim else 1
+        d.extensions[i] = float(extensions[i]) if (extensions is not None and i < dim) else 1.0
+    d.embedding_factor = embedding_factor
+    d.periodic = int(bool(periodic))
+    d.covariance = COVARIANCES[covariance] if isinstance(covariance, str) else int(covariance)
+    d.variance = variance
+    cl = np.atleast_1d(np.asarray(corr_length, dtype=np.float64)).ravel()
+    if anisotropy is None:
+        if cl.size == 1:
+            anisotropy = "none"
+        elif cl.size == dim:
+            anisotropy = "axiparallel"
+        elif cl.size == dim * dim:
+            anisotropy = "geometric"
+        else:
+            raise ValueError("stochastic.corrLength needs 1, dim or dim*dim values")
+    d.anisotropy = ANISOTROPIES[anisotropy] if isinstance(anisotropy, str) else int(anisotropy)
+    for i in range(9):
+        d.corr_length[i] = float(cl[i]) if i < cl.size else 0.0
+    d.matern_nu, d.exp_gamma = matern_nu, exp_gamma
+    d.cauchy_alpha, d.cauchy_beta = cauchy_alpha, cauchy_beta
+    d.approximate = int(bool(approximate))
+    d.threshold = threshold
+    d.transposed = transposed
+    d.matrix_backend = matrix_backend
+    d.field_backend = field_backend
+    d.precision = precision
+    d.eigen_check = eigen_check
+    d.cg_iterations = cg_iterations
+    d.transform = TRANSFORMS[transform] if isinstance(transform, str) else int(transform)
+    d.boxcox_lambda = boxcox_lambda
+    return d
+
+
+_lib = None
+
+
+def lib():
+    """Loads libpfcuda.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libpfcuda.so not built ({LIB_PATH}); run __graft_entry__.build()")
+    L = C.CDLL(LIB_PATH)
+    vp, u64, i32 = C.c_void_p, C.c_uint64, C.c_int32
+    sig = {
+        "pf_field_desc_init": (None, [C.POINTER(FieldDesc)]),
+        "pf_plan_create": (i32, [C.POINTER(FieldDesc), C.POINTER(vp)]),
+        "pf_plan_destroy": (None, [vp]),
+        "pf_plan_set_stream": (i32, [vp, vp]),
+        "pf_plan_get_info": (i32, [vp, C.POINTER(PlanInfo)]),
+        "pf_spectrum_build": (i32, [vp, C.POINTER(EigStats)]),
+        "pf_spectrum_copy": (i32, [vp, vp, u64]),
+        "pf_generate": (i32, [vp, vp, i32, u64, vp, i32, i32]),
+        "pf_generate_batch": (i32, [vp, u64, i32, vp, i32, i32]),
+        "pf_matvec": (i32, [vp, i32, i32, vp, vp, i32]),
+        "pf_multiply_inverse": (i32, [vp, vp, vp, i32, C.POINTER(CgOpts), C.POINTER(CgReport)]),
+        "pf_apply_transform": (i32, [vp, i32, vp, u64, i32]),
+        "pf_profile_enable": (i32, [vp, i32]),
+        "pf_profile_read": (i32, [vp, C.POINTER(KernelTime), i32, C.POINTER(i32)]),
+        "pf_launch_count": (u64, [vp]),
+        "pf_last_error_string": (C.c_char_p, []),
+        "pf_version": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+class PfError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"[pf status {status}] {msg}")
+        self.status = status
+
+
+class NegativeEigenvalueError(PfError):
+    """Mirror of parafields::NegativeEigenvalueError (exceptions.hh:8-15)."""
+
+
+def _check(st):
+    if st != PF_OK:
+        msg = lib().pf_last_error_string().decode()
+        if st == PF_ERR_NEG_EIGEN:
+            raise NegativeEigenvalueError(st, msg)
+        raise PfError(st, msg)
+
+
+def _ptr(a):
+    """(pointer, memory kind) for a numpy array or a torch CUDA tensor."""
+    if a is None:
+        return None, MEM_HOST
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data, MEM_HOST
+    # torch tensor
+    assert a.is_contiguous()
+    return a.data_ptr(), (MEM_DEVICE if a.is_cuda else MEM_HOST)
+
+
+class Plan:
+    """One field configuration on the GPU (the reference's Matrix object)."""
+
+    def __init__(self, desc: FieldDesc):
+        self.desc = desc
+        h = C.c_void_p()
+        _check(lib().pf_plan_create(C.byref(desc), C.byref(h)))
+        self.h = h
+        self.info = PlanInfo()
+        _check(lib().pf_plan_get_info(self.h, C.byref(self.info)))
+
+    def close(self):
+        if self.h:
+            lib().pf_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def domain_shape(self):
+        """numpy shape of a field (dimension 0 fastest => reversed)."""
+        return tuple(self.info.cells[i] for i in reversed(range(self.info.dim)))
+
+    def set_stream(self, stream_handle: int):
+        _check(lib().pf_plan_set_stream(self.h, C.c_void_p(stream_handle)))
+
+    def spectrum_build(self):
+        st = EigStats()
+        _check(lib().pf_spectrum_build(self.h, C.byref(st)))
+        return st.as_dict()
+
+    def spectrum(self):
+        out = np.empty(self.info.spectrum_size, dtype=np.float64)
+        _check(lib().pf_spectrum_copy(self.h, out.ctypes.data, out.size))
+        return out
+
+    def _field_dtype(self, precision=None):
+        p = self.info.precision if precision is None else precision
+        return np.float64 if p == PREC_F64 else np.float32
+
+    def generate(self, noise=None, seed=0, out=None, apply_transform=False):
+        if out is None:
+            out = np.empty(self.info.domain_size, dtype=self._field_dtype())
+        nptr, nmem = _ptr(noise)
+        optr, omem = _ptr(out)
+        _check(lib().pf_generate(self.h, nptr, nmem, seed, optr, omem, int(apply_transform)))
+        return out
+
+    def generate_batch(self, seed, count, out=None, apply_transform=False):
+        if out is None:
+            out = np.empty(self.info.domain_size * count, dtype=self._field_dtype())
+        optr, omem = _ptr(out)
+        _check(lib().pf_generate_batch(self.h, seed, count, optr, omem, int(apply_transform)))
+        return out
+
+    def matvec(self, x, op=OP_MUL, precision=PREC_F64, out=None):
+        if out is None:
+            out = np.empty_like(x)
+        iptr, mem = _ptr(x)
+        optr, _ = _ptr(out)
+        _check(lib().pf_matvec(self.h, op, precision, iptr, optr, mem))
+        return out
+
+    def multiply_inverse(self, b, x=None, mode=CG_REFERENCE, tolerance=1e-8, max_iterations=0,
+                         inner_fp32=False, precondition=True):
+        if x is None:
+            x = np.empty_like(b)
+        opts = CgOpts(mode, max_iterations, tolerance, int(inner_fp32), int(precondition))
+        rep = CgReport()
+        bptr, mem = _ptr(b)
+        xptr, _ = _ptr(x)
+        _check(lib().pf_multiply_inverse(self.h, bptr, xptr, mem, C.byref(opts), C.byref(rep)))
+        return x, {"iterations": rep.iterations, "refinements": rep.refinements,
+                   "relative_residual": rep.relative_residual}
+
+    def apply_transform(self, data, precision=PREC_F64):
+        ptr, mem = _ptr(data)
+        n = data.size if isinstance(data, np.ndarray) else data.numel()
+        _check(lib().pf_apply_transform(self.h, precision, ptr, n, mem))
+        return data
+
+    def profile(self, enable=True):
+        _check(lib().pf_profile_enable(self.h, int(enable)))
+
+    def profile_read(self):
+        cap = 64
+        arr = (KernelTime * cap)()
+        n = C.c_int32()
+        _check(lib().pf_profile_read(self.h, arr, cap, C.byref(n)))
+        return [{"name": arr[i].name.decode(), "launches": arr[i].launches,
+                 "total_ms": arr[i].total_ms, "bytes": arr[i].bytes} for i in range(n.value)]
+
+    def launch_count(self):
+        return int(lib().pf_launch_count(self.h))

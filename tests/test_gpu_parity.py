@@ -1,0 +1,206 @@
+"""GPU parity: libpfcuda.so (through the C ABI) against the FP64 oracle on identical
+seeded noise.  Tolerances (relative L2 unless stated):
+  FP64 spectrum / field / matvec: 1e-12   (different FFT factorisations, both FP64)
+  FP32 field / matvec:            1e-5    (FP32 transforms of an FP64 spectrum)
+  eigenvalue statistics:          exact counts, smallest to 1e-12 relative
+"""
+import numpy as np
+import pytest
+
+import pfb200
+from helpers import desc_of, rel
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+
+CONFIGS = {
+    "2d-exp-iso": dict(dim=2, cells=(64, 48), covariance="exponential", corr_length=0.1),
+    "2d-cubic-axi": dict(dim=2, cells=(40, 72), covariance="cubic", corr_length=(0.3, 0.2),
+                         anisotropy="axiparallel", extensions=(1.0, 2.0)),
+    "2d-sph-geo": dict(dim=2, cells=(50, 36), covariance="spherical", corr_length=(0.2, 0.05, -0.05, 0.15),
+                       anisotropy="geometric", approximate=True),
+    "2d-gauss-geo": dict(dim=2, cells=(48, 48), covariance="gaussian", corr_length=(0.06, 0.0, 0.0, 0.04),
+                         anisotropy="geometric"),
+    "3d-matern32-axi": dict(dim=3, cells=(32, 24, 20), covariance="matern32", corr_length=(0.2, 0.1, 0.05),
+                            anisotropy="axiparallel"),
+    "3d-exp-geo": dict(dim=3, cells=(24, 20, 16), covariance="exponential",
+                       corr_length=(0.15, 0.02, 0.0, -0.03, 0.08, 0.01, 0.0, 0.02, 0.04), anisotropy="geometric",
+                       approximate=True),
+    "3d-gexp-iso-notransp": dict(dim=3, cells=(16, 20, 24), covariance="gammaExponential", exp_gamma=1.3,
+                                 corr_length=0.1, transposed=0),
+}
+
+
+def plan_and_oracle(oracle, cfg, **over):
+    d = desc_of(cfg, **over)
+    P = pfb200.Plan(d)
+    lam, st, status = oracle.spectrum(d)
+    return d, P, lam, st, status
+
+
+@pytest.mark.parametrize("name", list(CONFIGS))
+def test_spectrum_and_stats(oracle, name):
+    d, P, lam, st, status = plan_and_oracle(oracle, CONFIGS[name])
+    assert status == 0
+    gst = P.spectrum_build()
+    glam = P.spectrum()
+    assert rel(glam, lam) < TOL64
+    assert (gst["small"], gst["zero"], gst["negative"]) == (st["small"], st["zero"], st["negative"])
+    assert abs(gst["smallest"] - st["smallest"]) <= 1e-12 * max(abs(st["smallest"]), 1e-300) + 1e-18
+
+
+def test_reference_eigen_scan_mode(oracle):
+    cfg = dict(dim=2, cells=(32, 32), covariance="gaussian", corr_length=(0.5, 0.0, 0.0, 0.5),
+               anisotropy="geometric", approximate=True)
+    for mode in (pfb200.EIGCHECK_CORRECTED, pfb200.EIGCHECK_REFERENCE):
+        d, P, lam, st, _ = plan_and_oracle(oracle, cfg, eigen_check=mode)
+        gst = P.spectrum_build()
+        assert (gst["small"], gst["zero"], gst["negative"]) == (st["small"], st["zero"], st["negative"])
+        assert rel(P.spectrum(), lam) < TOL64
+
+
+def test_negative_eigenvalues_raise(oracle):
+    cfg = dict(dim=2, cells=(32, 32), covariance="gaussian", corr_length=0.5)
+    P = pfb200.Plan(desc_of(cfg))
+    with pytest.raises(pfb200.NegativeEigenvalueError, match="negative eigenvalues"):
+        P.spectrum_build()
+
+
+@pytest.mark.parametrize("prec", [pfb200.PREC_F64, pfb200.PREC_F32])
+@pytest.mark.parametrize("name", list(CONFIGS))
+def test_generate_parity(oracle, name, prec):
+    d, P, lam, st, _ = plan_and_oracle(oracle, CONFIGS[name], precision=prec)
+    g = oracle.resolve(d)
+    noise = oracle.noise(20261203, g.noise)
+    ref, _ = oracle.generate(d, lam, noise)
+    out = P.generate(noise=noise)
+    assert rel(out, ref) < (TOL64 if prec == pfb200.PREC_F64 else TOL32)
+
+
+@pytest.mark.parametrize("prec", [pfb200.PREC_F64, pfb200.PREC_F32])
+@pytest.mark.parametrize("op", [pfb200.OP_MUL, pfb200.OP_ROOT, pfb200.OP_INVEXT])
+@pytest.mark.parametrize("name", ["2d-exp-iso", "2d-sph-geo", "3d-matern32-axi", "3d-exp-geo"])
+def test_matvec_parity(oracle, name, op, prec):
+    d, P, lam, st, _ = plan_and_oracle(oracle, CONFIGS[name])
+    g = oracle.resolve(d)
+    x = np.random.default_rng(5).standard_normal(g.domain)
+    ref = oracle.matvec(d, lam, op, x)
+    dt = np.float64 if prec == pfb200.PREC_F64 else np.float32
+    out = P.matvec(x.astype(dt), op=op, precision=prec)
+    assert rel(out, ref) < (TOL64 if prec == pfb200.PREC_F64 else TOL32)
+
+
+@pytest.mark.parametrize("name", ["2d-exp-iso", "3d-exp-geo"])
+def test_cg_reference_mode(oracle, name):
+    d, P, lam, st, _ = plan_and_oracle(oracle, CONFIGS[name], cg_iterations=40)
+    g = oracle.resolve(d)
+    b = np.random.default_rng(9).standard_normal(g.domain)
+    xo, its = oracle.multiply_inverse(d, lam, b)
+    x, rep = P.multiply_inverse(b, mode=pfb200.CG_REFERENCE)
+    assert abs(rep["iterations"] - its) <= 1
+    assert rel(x, xo) < 1e-8
+
+
+@pytest.mark.parametrize("inner_fp32", [False, True])
+def test_cg_residual_mode(oracle, inner_fp32):
+    d, P, lam, st, _ = plan_and_oracle(oracle, CONFIGS["3d-matern32-axi"])
+    g = oracle.resolve(d)
+    b = np.random.default_rng(11).standard_normal(g.domain)
+    x, rep = P.multiply_inverse(b, mode=pfb200.CG_RESIDUAL, tolerance=1e-8, inner_fp32=inner_fp32)
+    assert rep["relative_residual"] <= 1e-8
+    # the oracle's FP64 matvec confirms the residual
+    assert rel(oracle.matvec(d, lam, pfb200.OP_MUL, x), b) <= 1.1e-8
+
+
+def test_cg_zero_rhs():
+    P = pfb200.Plan(desc_of(CONFIGS["2d-exp-iso"]))
+    b = np.zeros(64 * 48)
+    x, rep = P.multiply_inverse(b)
+    assert rep["iterations"] == 0 and not x.any()
+
+
+@pytest.mark.parametrize("kind", ["logNormal", "foldedNormal", "sign", "boxCox"])
+def test_generate_with_transform(oracle, kind):
+    cfg = dict(CONFIGS["2d-exp-iso"], transform=kind, boxcox_lambda=0.2)
+    d, P, lam, st, _ = plan_and_oracle(oracle, cfg)
+    g = oracle.resolve(d)
+    noise = oracle.noise(3, g.noise)
+    ref, _ = oracle.generate(d, lam, noise)
+    ref = oracle.transform(kind, ref, boxcox_lambda=0.2)
+    out = P.generate(noise=noise, apply_transform=True)
+    if kind == "sign":
+        assert (out == ref).mean() > 0.999
+    else:
+        assert rel(out, ref) < 1e-11
+    v = np.random.default_rng(4).standard_normal(1000) * 0.3
+    np.testing.assert_allclose(P.apply_transform(v.copy()), oracle.transform(kind, v, boxcox_lambda=0.2),
+                               rtol=1e-13)
+
+
+def test_1d_dft_backend_and_spare_field(oracle):
+    cfg = dict(dim=1, cells=(96,), covariance="exponential", corr_length=0.05)
+    d, P, lam, st, _ = plan_and_oracle(oracle, cfg)
+    assert P.info.matrix_backend == pfb200.MATRIX_DFT and P.info.field_backend == pfb200.FIELD_DFT
+    g = oracle.resolve(d)
+    noise = oracle.noise(1, g.noise)
+    ref, spare = oracle.generate(d, lam, noise)
+    out1 = P.generate(noise=noise)
+    out2 = P.generate(noise=oracle.noise(2, g.noise))  # returns the cached second field
+    assert rel(P.spectrum(), lam) < TOL64
+    assert rel(out1, ref) < TOL64 and rel(out2, spare) < TOL64
+    x = np.random.default_rng(3).standard_normal(g.domain)
+    assert rel(P.matvec(x), oracle.matvec(d, lam, pfb200.OP_MUL, x)) < TOL64
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_dft_matrix_and_field_backends(oracle, dim):
+    cells = (24, 20) if dim == 2 else (12, 10, 8)
+    cfg = dict(dim=dim, cells=cells, covariance="matern52", corr_length=0.15,
+               matrix_backend=pfb200.MATRIX_DFT, field_backend=pfb200.FIELD_DFT)
+    d, P, lam, st, _ = plan_and_oracle(oracle, cfg)
+    g = oracle.resolve(d)
+    assert rel(P.spectrum() if P.spectrum_build() is not None else None, lam) < TOL64
+    noise = oracle.noise(5, g.noise)
+    ref, spare = oracle.generate(d, lam, noise)
+    assert rel(P.generate(noise=noise), ref) < TOL64
+    assert rel(P.generate(noise=noise), spare) < TOL64
+    x = np.random.default_rng(3).standard_normal(g.domain)
+    for op in (pfb200.OP_MUL, pfb200.OP_ROOT, pfb200.OP_INVEXT):
+        assert rel(P.matvec(x, op=op), oracle.matvec(d, lam, op, x)) < TOL64
+
+
+def test_device_pointers(oracle):
+    torch = pytest.importorskip("torch")
+    d, P, lam, st, _ = plan_and_oracle(oracle, CONFIGS["3d-matern32-axi"], precision=pfb200.PREC_F32)
+    g = oracle.resolve(d)
+    noise = oracle.noise(8, g.noise)
+    ref, _ = oracle.generate(d, lam, noise)
+    nd = torch.from_numpy(noise).cuda()
+    out = torch.empty(g.domain, dtype=torch.float32, device="cuda")
+    P.generate(noise=nd, out=out)
+    torch.cuda.synchronize()
+    assert rel(out.cpu().numpy(), ref) < TOL32
+    x = torch.randn(g.domain, dtype=torch.float32, device="cuda")
+    y = torch.empty_like(x)
+    P.matvec(x, precision=pfb200.PREC_F32, out=y)
+    torch.cuda.synchronize()
+    assert rel(y.cpu().numpy(), oracle.matvec(d, lam, pfb200.OP_MUL, x.cpu().double().numpy())) < TOL32
+
+
+def test_counter_based_noise_statistics(oracle):
+    """Seeded on-device noise: the empirical covariance of many realizations matches the
+    exact covariance of the reference's generator (J J^T, J = d field / d noise,
+    computed with the oracle from unit noise vectors)."""
+    cfg = dict(dim=2, cells=(8, 6), covariance="exponential", corr_length=0.3)
+    d, P, lam, st, _ = plan_and_oracle(oracle, cfg)
+    g = oracle.resolve(d)
+    J = np.stack([oracle.generate(d, lam, np.eye(g.noise)[i])[0] for i in range(g.noise)], axis=1)
+    exact = J @ J.T
+    M = 20000
+    fields = P.generate_batch(seed=123, count=M).reshape(M, g.domain)
+    emp = fields.T @ fields / M
+    se = np.sqrt((np.diag(exact)[:, None] * np.diag(exact)[None, :] + exact ** 2) / M)
+    assert np.abs(fields.mean(axis=0)).max() < 5 * np.sqrt(np.diag(exact).max() / M)
+    assert (np.abs(emp - exact) < 5 * se + 1e-12).mean() > 0.995

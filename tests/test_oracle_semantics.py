@@ -1,0 +1,168 @@
+"""The FP64 oracle against an independent numpy/scipy restatement and against the
+analytic properties of circulant embedding (matrix.hh:223-421, 1315-1646)."""
+import numpy as np
+import pytest
+
+import npref
+import pfb200
+from helpers import desc_of, full_lambda, rel
+
+CASES_2D = [
+    dict(dim=2, cells=(16, 12), covariance=c, corr_length=0.15, anisotropy="none")
+    for c in ["exponential", "gaussian", "spherical", "separableExponential", "matern32", "matern52",
+              "dampedOscillation", "cauchy", "cubic", "whiteNoise"]
+] + [
+    dict(dim=2, cells=(16, 12), covariance="gammaExponential", exp_gamma=1.5, corr_length=0.15),
+    dict(dim=2, cells=(16, 12), covariance="generalizedCauchy", cauchy_alpha=1.2, cauchy_beta=2.0,
+         corr_length=0.15),
+    dict(dim=2, cells=(20, 14), covariance="exponential", corr_length=(0.2, 0.07), anisotropy="axiparallel",
+         extensions=(2.0, 1.0)),
+    dict(dim=2, cells=(18, 16), covariance="matern52", corr_length=(0.2, 0.05, -0.03, 0.1),
+         anisotropy="geometric", approximate=True),
+]
+CASES_3D = [
+    dict(dim=3, cells=(8, 6, 10), covariance=c, corr_length=(0.2, 0.1, 0.15), anisotropy="axiparallel")
+    for c in ["exponential", "matern32", "spherical", "gaussian"]
+] + [
+    dict(dim=3, cells=(8, 6, 10), covariance="exponential",
+         corr_length=(0.15, 0.02, 0.0, -0.03, 0.1, 0.01, 0.0, 0.02, 0.12), anisotropy="geometric",
+         approximate=True),
+]
+
+
+@pytest.mark.parametrize("cfg", CASES_2D + CASES_3D, ids=lambda c: f"{c['dim']}d-{c['covariance']}-{c.get('anisotropy')}")
+def test_spectrum_matches_numpy(oracle, cfg):
+    d = desc_of(cfg)
+    g = oracle.resolve(d)
+    lam, stats, st = oracle.spectrum(d)
+    ref = npref.spectrum_full(cfg)
+    ref_clamped = np.where(ref < 0, 0.0, ref)
+    got = full_lambda(g, lam)
+    assert np.abs(got - ref_clamped).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("transposed", [-1, 0])
+@pytest.mark.parametrize("cfg", CASES_2D[:3] + CASES_3D[:2] + [CASES_2D[-1], CASES_3D[-1]],
+                         ids=lambda c: f"{c['dim']}d-{c['covariance']}-{c.get('anisotropy')}")
+def test_generate_matches_numpy(oracle, cfg, transposed):
+    d = desc_of(cfg, transposed=transposed)
+    g = oracle.resolve(d)
+    lam, stats, st = oracle.spectrum(d)
+    noise = oracle.noise(7, g.noise)
+    field, _ = oracle.generate(d, lam, noise)
+    ref = npref.generate_r2c(cfg, full_lambda(g, lam), noise, bool(g.transposed))
+    assert rel(field, ref) < 1e-12
+
+
+@pytest.mark.parametrize("op", [pfb200.OP_MUL, pfb200.OP_ROOT, pfb200.OP_INVEXT])
+@pytest.mark.parametrize("cfg", [CASES_2D[0], CASES_2D[-2], CASES_3D[0], CASES_3D[-1]],
+                         ids=lambda c: f"{c['dim']}d-{c.get('anisotropy')}")
+def test_matvec_matches_numpy(oracle, cfg, op):
+    d = desc_of(cfg)
+    g = oracle.resolve(d)
+    lam, _, _ = oracle.spectrum(d)
+    x = np.random.default_rng(1).standard_normal(g.domain)
+    y = oracle.matvec(d, lam, op, x)
+    shape = tuple(reversed(cfg["cells"][: cfg["dim"]]))
+    ref = npref.matvec(cfg, full_lambda(g, lam), x.reshape(shape), op)
+    assert rel(y, ref) < 1e-12
+
+
+def test_eigenvalues_sum_to_variance(oracle):
+    # classical embedding without clamping: sum_k lambda_k = c(0) = sigma^2
+    cfg = dict(dim=2, cells=(32, 24), covariance="exponential", corr_length=0.1, variance=1.7)
+    d = desc_of(cfg)
+    g = oracle.resolve(d)
+    lam, stats, st = oracle.spectrum(d)
+    assert st == 0 and stats["negative"] == 0
+    assert abs(full_lambda(g, lam).sum() - 1.7) < 1e-12
+
+
+def test_unit_vector_matvec_is_scaled_covariance_column(oracle):
+    # operator* returns (C x)/N (r2cmatrixbackend.hh:279-282 + r2cfieldbackend.hh:233-236)
+    cfg = dict(dim=2, cells=(16, 12), covariance="gaussian", corr_length=0.2)
+    d = desc_of(cfg)
+    g = oracle.resolve(d)
+    lam, _, _ = oracle.spectrum(d)
+    x = np.zeros(g.domain)
+    x[5 + 16 * 3] = 1.0
+    y = oracle.matvec(d, lam, pfb200.OP_MUL, x).reshape(12, 16)
+    c = npref.torus(cfg)
+    ref = np.array([[c[(j1 - 3) % c.shape[0], (j0 - 5) % c.shape[1]] for j0 in range(16)] for j1 in range(12)])
+    assert np.abs(y - ref / g.N).max() < 1e-15
+
+
+def test_cg_inverse(oracle):
+    cfg = dict(dim=2, cells=(16, 12), covariance="exponential", corr_length=0.1)
+    d = desc_of(cfg)
+    lam, _, _ = oracle.spectrum(d)
+    b = np.random.default_rng(0).standard_normal(16 * 12)
+    x, its = oracle.multiply_inverse(d, lam, b)
+    assert 0 < its <= 100
+    assert rel(oracle.matvec(d, lam, pfb200.OP_MUL, x), b) < 1e-8
+    # zero right-hand side is returned unchanged (matrix.hh:193-205)
+    z, its0 = oracle.multiply_inverse(d, lam, np.zeros(16 * 12))
+    assert its0 == 0 and not z.any()
+
+
+def test_reference_eigen_scan_defect(oracle):
+    # R2C real-view scan (r2cmatrixbackend.hh:164-170, 378-400): only the first N_c
+    # doubles (= N_c/2 complex entries) are checked; compare both modes with numpy
+    cfg = dict(dim=2, cells=(16, 16), covariance="gaussian", corr_length=(0.5, 0.0, 0.0, 0.5),
+               anisotropy="geometric", approximate=True)
+    lam_c, st_c, _ = oracle.spectrum(desc_of(cfg, eigen_check=pfb200.EIGCHECK_CORRECTED))
+    lam_r, st_r, _ = oracle.spectrum(desc_of(cfg, eigen_check=pfb200.EIGCHECK_REFERENCE))
+    c = npref.torus(cfg)
+    X = np.fft.rfftn(c) / c.size
+    flat = X.ravel()
+    re = flat.real
+    assert st_c["negative"] == int((re <= -1e-14).sum()) and st_c["negative"] > 0
+    view = np.stack([flat.real, flat.imag], axis=-1).ravel()[: flat.size]
+    assert st_r["negative"] == int((view <= -1e-14).sum())
+    assert st_r["smallest"] == view.min()
+    # corrected mode clamps every negative real part; the reference mode leaves the
+    # second half unclamped
+    assert (lam_c >= 0).all()
+    half = flat.size // 2
+    assert (lam_r[half + 1:] < 0).any()
+    np.testing.assert_allclose(lam_r[half + 1:], re[half + 1:], rtol=0, atol=1e-15)
+
+
+def test_negative_eigenvalue_status(oracle):
+    cfg = dict(dim=2, cells=(16, 16), covariance="gaussian", corr_length=0.5)
+    _, st, status = oracle.spectrum(desc_of(cfg))
+    assert st["negative"] > 0 and status == pfb200.PF_ERR_NEG_EIGEN
+    _, _, status = oracle.spectrum(desc_of(cfg, approximate=True))
+    assert status == 0
+
+
+@pytest.mark.parametrize("kind", ["none", "logNormal", "foldedNormal", "sign", "boxCox"])
+def test_value_transforms(oracle, kind):
+    v = np.random.default_rng(2).standard_normal(1000) * 0.5
+    out = oracle.transform(kind, v, boxcox_lambda=0.3)
+    ref = {"none": v, "logNormal": np.exp(v), "foldedNormal": np.abs(v),
+           "sign": np.where(v < 0, -1.0, 1.0), "boxCox": (v * 0.3 + 1) ** -0.3}[kind]
+    np.testing.assert_allclose(out, ref, rtol=1e-15)
+
+
+@pytest.mark.parametrize("over,msg", [
+    (dict(dim=3, cells=(4, 4, 4), covariance="cubic", corr_length=0.1), "cubic"),
+    (dict(covariance="gammaExponential", exp_gamma=2.5), "gamma"),
+    (dict(covariance="generalizedCauchy", cauchy_alpha=3.0), "alpha"),
+    (dict(covariance="matern"), "gsl"),
+])
+def test_config_errors(oracle, over, msg):
+    cfg = dict(dim=2, cells=(8, 8), covariance="exponential", corr_length=0.1)
+    cfg.update(over)
+    with pytest.raises(ValueError, match=msg):
+        oracle.resolve(desc_of(cfg))
+
+
+def test_default_backends_and_layout(oracle):
+    g = oracle.resolve(desc_of(dict(dim=2, cells=(8, 8), covariance="exponential", corr_length=0.1)))
+    assert (g.matrix_backend, g.field_backend, g.transposed) == (pfb200.MATRIX_DCT, pfb200.FIELD_R2C, 0)
+    g = oracle.resolve(desc_of(dict(dim=3, cells=(8, 6, 4), covariance="exponential", corr_length=0.1)))
+    assert (g.matrix_backend, g.field_backend, g.transposed) == (pfb200.MATRIX_DCT, pfb200.FIELD_R2C, 1)
+    assert list(g.Ts) == [16, 8, 12]
+    g = oracle.resolve(desc_of(dict(dim=1, cells=(32,), covariance="exponential", corr_length=0.1)))
+    assert (g.matrix_backend, g.field_backend, g.transposed) == (pfb200.MATRIX_DFT, pfb200.FIELD_DFT, 0)
