@@ -175,7 +175,7 @@ struct pf_plan {
   double* sq64 = nullptr;
   float* sq32 = nullptr;
   float* lam32 = nullptr;
-  void* fac[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  void* fac[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
   ScanOut* scan = nullptr;
   // workspaces
   void* ws[3] = {nullptr, nullptr, nullptr};
@@ -489,7 +489,7 @@ static pf_status build_spectrum(pf_plan* P) {
   const pf_field_desc* d = &P->desc;
   TRY(spectrum_alloc(P));
   for (int a = 0; a < 2; a++)
-    for (int o = 0; o < 3; o++)
+    for (int o = 0; o < 4; o++)
       if (P->fac[a][o]) {
         cudaFree(P->fac[a][o]);
         P->bytes_held -= g.S * (a == 0 ? 8 : 4);
@@ -548,7 +548,8 @@ static pf_status build_spectrum(pf_plan* P) {
     }
   }
   // eigenvalue scan, clamp, square roots
-  CK(cudaMemsetAsync(P->scan, 0, sizeof(ScanOut), P->stream));
+  static const ScanOut scan_init = {0u, 0u, 0u, 0u, ~0ull};  // min key starts at the largest key
+  CK(cudaMemcpyAsync(P->scan, &scan_init, sizeof(ScanOut), cudaMemcpyHostToDevice, P->stream));
   ScanArgs sa{};
   sa.spec = spec;
   for (int i = 0; i < 3; i++) {
@@ -841,6 +842,10 @@ static pf_status matvec_dev(pf_plan* P, int op, const S* in, S* out) {
   return matvec_dft<T, S>(P, op, in, out);
 }
 
+// internal operation: torus pseudo-inverse (clamped eigenvalues dropped), used as the
+// preconditioner of the residual-mode CG
+constexpr int kOpInvPinv = 3;
+
 // CG helpers use FP64 vectors with FP64 or FP32 transforms
 static pf_status cg_matvec(pf_plan* P, int op, bool fp32, const double* in, double* out) {
   if (fp32) return matvec_dev<float, double>(P, op, in, out);
@@ -939,7 +944,7 @@ void pf_plan_destroy(pf_plan* P) {
   for (void** b : bufs)
     if (*b) cudaFree(*b), *b = nullptr;
   for (int a = 0; a < 2; a++)
-    for (int o = 0; o < 3; o++)
+    for (int o = 0; o < 4; o++)
       if (P->fac[a][o]) cudaFree(P->fac[a][o]);
   for (auto& kv : P->tw) cudaFree(kv.second);
   cg_free(P);

@@ -733,7 +733,7 @@ __global__ void __launch_bounds__(kThreads) k_scan(const ScanArgs a) {
 // (dftmatrixbackend.hh:322-338); same statistics as above.
 // (covered by k_scan with faithful = 0 over the full complex torus.)
 
-// factor arrays for the matvecs: lambda/N, sqrt(lambda)/N, 1/(lambda N)
+// factor arrays for the matvecs: lambda/N, sqrt(lambda)/N, 1/(lambda N), pinv(lambda)/N
 template <typename T>
 __global__ void k_factors(const double* __restrict__ lam, uint64_t n, double invN, int op, T* out) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -743,8 +743,10 @@ __global__ void k_factors(const double* __restrict__ lam, uint64_t n, double inv
       f = l * invN;
     else if (op == 1)
       f = sqrt(l) * invN;
-    else
+    else if (op == 2)
       f = (1. / l) * invN;
+    else  // pseudo-inverse: clamped (zero) eigenvalues are left out of the preconditioner
+      f = l > 0. ? (1. / l) * invN : 0.;
     out[i] = (T)f;
   }
 }
