@@ -248,6 +248,21 @@ pf_status pf_generate_batch(pf_plan* plan, uint64_t seed, int32_t count, void* o
 pf_status pf_matvec(pf_plan* plan, int32_t op, int32_t precision, const void* in, void* out,
                     int32_t mem);
 
+/* FP64 matrix-vector product (as pf_matvec with PF_PREC_F64) that allocates no memory.
+ * No counterpart in the reference: it exists for callers that may not call cudaMalloc
+ * when they need the product -- code living inside another framework's memory pool,
+ * solvers that reserve all device memory at start-up and cannot afford the device
+ * synchronization of a later allocation, and callbacks that run during stream capture.
+ * Limits: 2D plans with the R2C field backend, spectrum already built (PF_ERR_STATE
+ * otherwise), `in`/`out` are device pointers of prod(cells) doubles, and the scratch
+ * (T0/2+1)*n1 + T0/2 + T0 + T1 complex doubles must fit in the library's fixed
+ * 2^18-element (4 MiB) device array (PF_ERR_ARG otherwise).  That array lives in every
+ * GPU that loads the library until the process exits; the first call on a device looks
+ * up its address (make that call before any stream capture).  Calls share the array:
+ * calls that overlap on the GPU race and must be serialized.  Asynchronous on the plan's
+ * stream. */
+pf_status pf_matvec_static(pf_plan* plan, int32_t op, const double* in, double* out);
+
 /* Matrix::multiplyInverse (matrix.hh:189-206): zero-input shortcut, torus-inverse
  * initial guess, then the preconditioned CG of innerCG (matrix.hh:1315-1432).
  * FP64 vectors; `opts` NULL = reference mode. */

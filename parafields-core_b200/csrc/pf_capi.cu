@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1197,3 +1198,156 @@ const char* pf_last_error_string(void) { return g_err.c_str(); }
 const char* pf_version(void) { return "parafields-b200 0.1 (sm_100a)"; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Matrix-vector product without any device allocation
+//
+// Some callers cannot allocate device memory at the moment they need a product with
+// the covariance: code running inside another framework's memory pool (which may
+// own all of the GPU's memory), solvers that reserve their memory once at start-up
+// and treat a later cudaMalloc as an error because it synchronizes the device, or
+// callbacks that run while a stream is being captured.  For them this variant of
+// the 2D matvec keeps its scratch (the half-spectrum torus and the twiddle tables)
+// in one fixed array that is part of the library image, so a call allocates nothing.
+//
+// The array is a file-scope __device__ symbol: every GPU that loads the library holds
+// it until the process exits.  Its host-side name is only a stand-in, so the device
+// address is fetched with cudaGetSymbolAddress once per device, on the first call made
+// with that device current; make that first call before any stream capture starts.
+// All calls share the array and every call rewrites the parts it reads, so nothing in
+// it has to start at zero; calls that overlap on the GPU (other streams, other plans,
+// other threads) race on it and must be serialized by the caller.
+// ---------------------------------------------------------------------------
+constexpr size_t kStaticScratchElems = size_t(1) << 18;  // complex doubles: 4 MiB
+static __device__ __align__(256) double2 g_static_scratch[kStaticScratchElems];
+
+static std::mutex g_static_mutex;
+static double2* g_static_addr[128] = {nullptr};
+
+static pf_status static_scratch_address(double2** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return fail(PF_ERR_ARG, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (!g_static_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) return fail(PF_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+    g_static_addr[dev] = (double2*)p;
+  }
+  *out = g_static_addr[dev];
+  return PF_OK;
+}
+
+// exp(-2 pi i m / L), m < L, into tw
+__global__ void k_static_twiddles(double2* tw, int L) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < L; m += gridDim.x * blockDim.x) {
+    double s, c;
+    sincospi(-2.0 * (double)m / (double)L, &s, &c);
+    tw[m] = make_double2(c, s);
+  }
+}
+
+// eigenvalue factor computed from the FP64 spectrum on the fly (no factor array)
+struct StaticMid {
+  static constexpr bool active = true;
+  int T0, T1, C0, layout, D0;
+  int op;
+  double N;
+  const double* lam;
+  long long nlam;
+  template <typename T>
+  __device__ __forceinline__ cx<T> operator()(long long p, int j, long long, cx<T> v) const {
+    const int k0 = (int)p, k1 = j;
+    long long li;
+    if (layout == 0) {
+      const int m1 = k1 <= T1 / 2 ? k1 : T1 - k1;
+      li = (long long)k0 + (long long)D0 * m1;
+    } else {
+      li = (long long)k0 + (long long)C0 * k1;
+    }
+    if (!in_bounds(li, nlam)) return mk<T>(0, 0);
+    const double l = lam[li];
+    const double f = op == 0 ? l / N : (op == 1 ? sqrt(l) / N : (1. / l) / N);
+    return mk<T>((T)(v.x * f), (T)(v.y * f));
+  }
+};
+
+extern "C" pf_status pf_matvec_static(pf_plan* P, int32_t op, const double* in, double* out) {
+  if (!P || !in || !out) return fail(PF_ERR_ARG, "null argument");
+  if (op < 0 || op > 2) return fail(PF_ERR_ARG, "unknown operation");
+  const Geom& g = P->g;
+  if (g.dim != 2 || g.fb != PF_FIELD_R2C)
+    return fail(PF_ERR_CONFIG, "pf_matvec_static serves 2D plans with the R2C field backend");
+  if (!P->have_spec) return fail(PF_ERR_STATE, "spectrum not built: call pf_spectrum_build first");
+  const int T0 = g.T[0], T1 = g.T[1], L0 = T0 / 2, T0c = g.T0c, n0 = g.n[0], n1 = g.n[1];
+  const size_t nX = (size_t)T0c * n1;
+  const size_t need = nX + (size_t)L0 + (size_t)T0 + (size_t)T1;
+  if (need > kStaticScratchElems)
+    return fail(PF_ERR_ARG, "field too large for the static scratch: needs %zu complex doubles, limit %zu", need,
+                kStaticScratchElems);
+  double2* base = nullptr;
+  TRY(static_scratch_address(&base));
+  double2* X = base;
+  double2* twL = X + nX;
+  double2* twT = twL + L0;
+  double2* tw1 = twT + T0;
+  k_static_twiddles<<<8, 256, 0, P->stream>>>(twL, L0);
+  k_static_twiddles<<<8, 256, 0, P->stream>>>(twT, T0);
+  k_static_twiddles<<<8, 256, 0, P->stream>>>(tw1, T1);
+  P->launches += 3;
+  CK(cudaGetLastError());
+  ArrStore<double2> xs{X, 1, 0, T0c, (long long)nX};
+  ArrLoad<double2> xl0{X, 1, 0, T0c, (long long)nX, T0c};
+  FieldRowLoad<double> fl{in, n0, (long long)g.domain};
+  FieldRowStore<double> fs{out, n0, 0, 0.0, (long long)g.domain};
+  // dimension 0 forward (r2c with zero padding)
+  PassArgs a{};
+  a.L = L0;
+  a.Lout = T0c;
+  a.npencil = n1;
+  a.nouter = 1;
+  a.sign = -1;
+  if (!make_radices(L0, &a.rad)) return fail(PF_ERR_CONFIG, "length %d has a prime factor above 13", T0);
+  tile_params(L0, 16, true, &a);
+  size_t smem = smem_of(a, true, 16);
+  if (smem > 227 * 1024) return fail(PF_ERR_CONFIG, "row of length %d does not fit in shared memory", T0);
+  {
+    auto kern = k_r2c<double, FieldRowLoad<double>, ArrStore<double2>>;
+    TRY(set_smem(kern, smem));
+    kern<<<(unsigned)((n1 + a.B - 1) / a.B), kThreads, smem, P->stream>>>(a, twL, twT, fl, xs);
+  }
+  // dimension 1: forward, eigenvalue factor, backward, in place
+  StaticMid mid{T0, T1, g.mb == PF_MATRIX_R2C ? T0c : T0, g.mb == PF_MATRIX_DCT ? 0 : 1, T0 / 2 + 1, op,
+                (double)g.N, P->lam64, (long long)g.S};
+  PassArgs b{};
+  b.L = T1;
+  b.Lout = n1;
+  b.npencil = T0c;
+  b.nouter = 1;
+  b.sign = -1;
+  b.sign2 = +1;
+  if (!make_radices(T1, &b.rad)) return fail(PF_ERR_CONFIG, "length %d has a prime factor above 13", T1);
+  tile_params(T1, 16, false, &b);
+  smem = smem_of(b, false, 16);
+  if (smem > 227 * 1024) return fail(PF_ERR_CONFIG, "pencil of length %d does not fit in shared memory", T1);
+  {
+    ArrLoad<double2> xl1{X, T0c, 0, 1, (long long)nX, n1};
+    ArrStore<double2> xs1{X, T0c, 0, 1, (long long)nX};
+    auto kern = k_pass<double, false, ArrLoad<double2>, StaticMid, ArrStore<double2>>;
+    TRY(set_smem(kern, smem));
+    kern<<<(unsigned)((T0c + b.B - 1) / b.B), kThreads, smem, P->stream>>>(b, tw1, xl1, mid, xs1);
+  }
+  // dimension 0 backward (c2r) with extraction of the domain
+  a.sign = +1;
+  a.Lout = n0;
+  smem = smem_of(a, true, 16);
+  {
+    auto kern = k_c2r<double, ArrLoad<double2>, FieldRowStore<double>>;
+    TRY(set_smem(kern, smem));
+    kern<<<(unsigned)((n1 + a.B - 1) / a.B), kThreads, smem, P->stream>>>(a, twL, twT, xl0, fs);
+  }
+  P->launches += 3;
+  CK(cudaGetLastError());
+  return PF_OK;
+}

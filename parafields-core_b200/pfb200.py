@@ -152,6 +152,7 @@ def lib():
         "pf_generate": (i32, [vp, vp, i32, u64, vp, i32, i32]),
         "pf_generate_batch": (i32, [vp, u64, i32, vp, i32, i32]),
         "pf_matvec": (i32, [vp, i32, i32, vp, vp, i32]),
+        "pf_matvec_static": (i32, [vp, i32, vp, vp]),
         "pf_multiply_inverse": (i32, [vp, vp, vp, i32, C.POINTER(CgOpts), C.POINTER(CgReport)]),
         "pf_apply_transform": (i32, [vp, i32, vp, u64, i32]),
         "pf_profile_enable": (i32, [vp, i32]),
