@@ -113,7 +113,10 @@ def test_cg_reference_mode(oracle, name):
     assert rep["iterations"] > 0 and its > 0
     assert rel(x, xo) < 1e-8
     r_gpu = rel(oracle.matvec(d, lam, pfb200.OP_MUL, x), b)
-    assert r_gpu < 1e-6
+    r_orc = rel(oracle.matvec(d, lam, pfb200.OP_MUL, xo), b)
+    # same algorithm, same quality: on the compactly supported cubic covariance the
+    # reference's 60 iterations stop far from convergence in both implementations
+    assert r_gpu <= 1.01 * r_orc + 1e-9
     assert abs(rep["relative_residual"] - r_gpu) <= 1e-3 * r_gpu + 1e-14
 
 
