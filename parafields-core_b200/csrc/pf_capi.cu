@@ -18,6 +18,7 @@
 #include "../../include/parafields_b200.h"
 #include "pf_cg.cuh"
 #include "pf_kernels.cuh"
+#include "pf_fastfft.cuh"
 
 using namespace pf;
 
@@ -388,6 +389,101 @@ static size_t cap_of(const pf_plan* P, const void* p) {
   return 0;
 }
 
+// compile-time specialised passes for the common lengths; other lengths fall back to
+// the runtime-radix kernels above
+template <typename T, int SIGN, int SIGN2, bool CONTIG, bool PAIR, class Ld, class Mid, class St, int L>
+static pf_status launch_fpass(pf_plan* P, const char* name, int Lout, long long npencil, long long nouter, Ld ld,
+                              Mid mid, St st, double bytes) {
+  constexpr int B = fast_B<T, L>();
+  PassArgs a{};
+  a.L = L;
+  a.Lout = Lout;
+  a.B = B;
+  a.npencil = npencil;
+  a.nouter = nouter;
+  a.sign = SIGN;
+  a.sign2 = SIGN2;
+  const cx<T>* tw = nullptr;
+  TRY(twiddles<T>(P, L, &tw));
+  const size_t smem = (size_t)(2 * L * B + L) * sizeof(cx<T>);
+  auto kern = k_fpass<T, L, B, SIGN, SIGN2, CONTIG, PAIR, Ld, Mid, St>;
+  TRY(set_smem(kern, smem));
+  const long long tiles = (npencil + B - 1) / B;
+  const long long grid = CONTIG ? tiles : tiles * nouter;
+  if (grid <= 0) return PF_OK;
+  if (grid > 0x7fffffffLL || npencil > 0x7fffffffLL) return fail(PF_ERR_CONFIG, "pass %s too large", name);
+  ProfRec rec;
+  TRY(prof_begin(P, name, bytes, &rec));
+  kern<<<(unsigned)grid, kThreads, smem, P->stream>>>(a, tw, ld, mid, st);
+  return prof_end(P, &rec);
+}
+
+#define PF_FAST_LENGTHS(X) X(64) X(128) X(256) X(512) X(1024) X(2048)
+
+template <typename T, int SIGN, int SIGN2, bool CONTIG, bool PAIR, class Ld, class Mid, class St>
+static pf_status run_fpass(pf_plan* P, const char* name, int L, int Lout, long long npencil, long long nouter, Ld ld,
+                           Mid mid, St st, double bytes) {
+  switch (L) {
+#define PF_CASE(LL) \
+  case LL:          \
+    return launch_fpass<T, SIGN, SIGN2, CONTIG, PAIR, Ld, Mid, St, LL>(P, name, Lout, npencil, nouter, ld, mid, st, bytes);
+    PF_FAST_LENGTHS(PF_CASE)
+#undef PF_CASE
+    default:
+      return run_pass<T, CONTIG>(P, name, L, Lout, npencil, nouter, SIGN, SIGN2, ld, mid, st, bytes);
+  }
+}
+
+template <typename T, bool R2C, class Ld, class St, int L>
+static pf_status launch_freal(pf_plan* P, const char* name, int Lout, long long rows, Ld ld, St st, double bytes) {
+  constexpr int B = fast_B<T, L>();
+  PassArgs a{};
+  a.L = L;
+  a.Lout = Lout;
+  a.B = B;
+  a.npencil = rows;
+  a.nouter = 1;
+  const cx<T>* tw = nullptr;
+  const cx<T>* twT = nullptr;
+  TRY(twiddles<T>(P, L, &tw));
+  TRY(twiddles<T>(P, 2 * L, &twT));
+  const size_t smem = (size_t)(2 * (L + 1) * B + 2 * L) * sizeof(cx<T>);
+  const long long grid = (rows + B - 1) / B;
+  if (grid <= 0) return PF_OK;
+  if (grid > 0x7fffffffLL || rows > 0x7fffffffLL) return fail(PF_ERR_CONFIG, "pass %s too large", name);
+  ProfRec rec;
+  if constexpr (R2C) {
+    auto kern = k_fr2c<T, L, B, Ld, St>;
+    TRY(set_smem(kern, smem));
+    TRY(prof_begin(P, name, bytes, &rec));
+    kern<<<(unsigned)grid, kThreads, smem, P->stream>>>(a, tw, twT, ld, st);
+  } else {
+    auto kern = k_fc2r<T, L, B, Ld, St>;
+    TRY(set_smem(kern, smem));
+    TRY(prof_begin(P, name, bytes, &rec));
+    kern<<<(unsigned)grid, kThreads, smem, P->stream>>>(a, tw, twT, ld, st);
+  }
+  return prof_end(P, &rec);
+}
+
+template <typename T, bool R2C, class Ld, class St>
+static pf_status run_freal(pf_plan* P, const char* name, int T0, int Lout, long long rows, Ld ld, St st,
+                           double bytes) {
+  switch (T0 / 2) {
+#define PF_CASE(LL) \
+  case LL:          \
+    return launch_freal<T, R2C, Ld, St, LL>(P, name, Lout, rows, ld, st, bytes);
+    PF_FAST_LENGTHS(PF_CASE)
+#undef PF_CASE
+    default:
+      return run_real_pass<T, R2C>(P, name, T0, Lout, rows, ld, st, bytes);
+  }
+}
+
+// row pitch of the half-spectrum work arrays: T0/2+1 rounded up to 8 complex, so every
+// B-wide segment of a strided pass starts on a 64-byte boundary
+static int half_pitch(const Geom& g) { return (g.T0c + 7) / 8 * 8; }
+
 template <typename S>
 static ArrLoad<S> arr_load(const pf_plan* P, const void* p, long long jstride, long long ostride, long long rowstride,
                            int Lin) {
@@ -639,7 +735,7 @@ static pf_status factor_array(pf_plan* P, int op, const T** out) {
 template <typename T, typename S>
 static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* out, int transform) {
   const Geom& g = P->g;
-  const int T0c = g.T0c;
+  const int T0c = g.T0c, P0 = half_pitch(g);
   R2CNoise nz{};
   nz.dim = g.dim;
   for (int i = 0; i < 3; i++) nz.ext[i] = g.T[i];
@@ -653,36 +749,43 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
   nz.seed = seed;
   nz.nsq = (long long)g.S;
   nz.nnoise = (long long)g.noise;
+  nz.Tl = g.T[g.dim - 1];
   FieldRowStore<S> fs{out, g.n[0], transform, P->desc.boxcox_lambda, (long long)g.domain};
   const double e = sizeof(cx<T>);
   const double noise_b = noise_dev ? 16.0 : 0.0;
   const double lam_b = sizeof(T);
+  const int last = g.dim - 1;
+  const int Tl = g.T[last];
+  void* W1 = nullptr;
   if (g.dim == 2) {
-    void* W1 = nullptr;
-    TRY(workspace(P, 0, sizeof(cx<T>) * (size_t)T0c * g.n[1], &W1));
-    // dimension 1 first: noise scaling fused into the load, output pruned to n1
-    TRY((run_pass<T, false>(P, "gen_noise_d1", g.T[1], g.n[1], T0c, 1, +1, +1, nz, NoMid(),
-                            arr_store<cx<T>>(P, W1, T0c, 0, 1),
-                            (double)T0c * g.T[1] * (noise_b + lam_b) + (double)T0c * g.n[1] * e)));
-    TRY((run_real_pass<T, false>(P, "gen_c2r_d0", g.T[0], g.n[0], g.n[1], arr_load<cx<T>>(P, W1, 1, 0, T0c, T0c), fs,
-                                 (double)g.n[1] * (T0c * e + g.n[0] * sizeof(S)))));
-    return PF_OK;
+    TRY(workspace(P, 0, sizeof(cx<T>) * (size_t)P0 * g.n[1], &W1));
+  } else {
+    TRY(workspace(P, 0, sizeof(cx<T>) * (size_t)P0 * g.T[1] * g.n[2], &W1));
   }
-  void *W1 = nullptr, *W2 = nullptr;
-  TRY(workspace(P, 0, sizeof(cx<T>) * (size_t)T0c * g.T[1] * g.n[2], &W1));
-  TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)T0c * g.n[1] * g.n[2], &W2));
-  const long long inner = (long long)T0c * g.T[1];
-  TRY((run_pass<T, false>(P, "gen_noise_d2", g.T[2], g.n[2], inner, 1, +1, +1, nz, NoMid(),
-                          arr_store<cx<T>>(P, W1, inner, 0, 1),
-                          (double)inner * g.T[2] * (noise_b + lam_b) + (double)inner * g.n[2] * e)));
-  TRY((run_pass<T, false>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, g.n[2], +1, +1,
-                          arr_load<cx<T>>(P, W1, T0c, inner, 1, g.T[1]), NoMid(),
-                          arr_store<cx<T>>(P, W2, T0c, (long long)T0c * g.n[1], 1),
-                          (double)T0c * g.n[2] * (g.T[1] + g.n[1]) * e)));
-  TRY((run_real_pass<T, false>(P, "gen_c2r_d0", g.T[0], g.n[0], (long long)g.n[1] * g.n[2],
-                               arr_load<cx<T>>(P, W2, 1, 0, T0c, T0c), fs,
-                               (double)g.n[1] * g.n[2] * (T0c * e + g.n[0] * sizeof(S)))));
-  return PF_OK;
+  // backward along the last dimension first, noise scaling fused into the load and the
+  // output pruned to the domain extent n_last (pencils: k0 x k1)
+  const long long outer = g.dim == 3 ? g.T[1] : 1;
+  const long long jst = g.dim == 3 ? (long long)P0 * g.T[1] : P0;
+  const double b1 = (double)T0c * outer * (Tl * (noise_b + lam_b) + (double)g.n[last] * e);
+  if (Tl % 2 == 0)
+    TRY((run_fpass<T, +1, +1, false, true>(P, "gen_noise_last", Tl, g.n[last], T0c, outer, nz, NoMid(),
+                                           arr_store<cx<T>>(P, W1, jst, P0, 1), b1)));
+  else
+    TRY((run_fpass<T, +1, +1, false, false>(P, "gen_noise_last", Tl, g.n[last], T0c, outer, nz, NoMid(),
+                                            arr_store<cx<T>>(P, W1, jst, P0, 1), b1)));
+  void* cur = W1;
+  if (g.dim == 3) {
+    void* W2 = nullptr;
+    TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)P0 * g.n[1] * g.n[2], &W2));
+    TRY((run_fpass<T, +1, +1, false, false>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, g.n[2],
+                                            arr_load<cx<T>>(P, W1, P0, (long long)P0 * g.T[1], 1, g.T[1]),
+                                            NoMid(), arr_store<cx<T>>(P, W2, P0, (long long)P0 * g.n[1], 1),
+                                            (double)T0c * g.n[2] * (g.T[1] + g.n[1]) * e)));
+    cur = W2;
+  }
+  const long long rows = g.dim == 3 ? (long long)g.n[1] * g.n[2] : g.n[1];
+  return run_freal<T, false>(P, "gen_c2r_d0", g.T[0], g.n[0], rows, arr_load<cx<T>>(P, cur, 1, 0, P0, T0c), fs,
+                             (double)rows * (T0c * e + g.n[0] * sizeof(S)));
 }
 
 // DFT field backend: complex noise on the whole torus, backward c2c on every axis,
@@ -756,40 +859,45 @@ static pf_status matvec_r2c(pf_plan* P, int op, const S* in, S* out) {
   const T* fac = nullptr;
   TRY(factor_array<T>(P, op, &fac));
   MultMid mid = mult_mid<T>(P, fac);
-  const int T0c = g.T0c;
+  const int T0c = g.T0c, P0 = half_pitch(g);
   const double e = sizeof(cx<T>);
   const double lb = sizeof(T);
   FieldRowLoad<S> fl{in, g.n[0], (long long)g.domain};
   FieldRowStore<S> fs{out, g.n[0], 0, 0.0, (long long)g.domain};
   if (g.dim == 2) {
     void* X1 = nullptr;
-    TRY(workspace(P, 2, sizeof(cx<T>) * (size_t)T0c * g.n[1], &X1));
-    TRY((run_real_pass<T, true>(P, "mv_r2c_d0", g.T[0], T0c, g.n[1], fl, arr_store<cx<T>>(P, X1, 1, 0, T0c),
-                                (double)g.n[1] * (g.n[0] * sizeof(S) + T0c * e))));
-    TRY((run_pass<T, false>(P, "mv_fused_d1", g.T[1], g.n[1], T0c, 1, -1, +1, arr_load<cx<T>>(P, X1, T0c, 0, 1, g.n[1]),
-                            mid, arr_store<cx<T>>(P, X1, T0c, 0, 1),
-                            (double)T0c * (2.0 * g.n[1] * e + g.T[1] * lb))));
-    return run_real_pass<T, false>(P, "mv_c2r_d0", g.T[0], g.n[0], g.n[1], arr_load<cx<T>>(P, X1, 1, 0, T0c, T0c), fs,
-                                   (double)g.n[1] * (T0c * e + g.n[0] * sizeof(S)));
+    TRY(workspace(P, 2, sizeof(cx<T>) * (size_t)P0 * g.n[1], &X1));
+    TRY((run_freal<T, true>(P, "mv_r2c_d0", g.T[0], T0c, g.n[1], fl, arr_store<cx<T>>(P, X1, 1, 0, P0),
+                            (double)g.n[1] * (g.n[0] * sizeof(S) + T0c * e))));
+    TRY((run_fpass<T, -1, +1, false, false>(P, "mv_fused_d1", g.T[1], g.n[1], T0c, 1,
+                                            arr_load<cx<T>>(P, X1, P0, 0, 1, g.n[1]), mid,
+                                            arr_store<cx<T>>(P, X1, P0, 0, 1),
+                                            (double)T0c * (2.0 * g.n[1] * e + g.T[1] * lb))));
+    return run_freal<T, false>(P, "mv_c2r_d0", g.T[0], g.n[0], g.n[1], arr_load<cx<T>>(P, X1, 1, 0, P0, T0c), fs,
+                               (double)g.n[1] * (T0c * e + g.n[0] * sizeof(S)));
   }
   void *X1 = nullptr, *X2 = nullptr;
-  TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)T0c * g.n[1] * g.n[2], &X1));
-  TRY(workspace(P, 2, sizeof(cx<T>) * (size_t)T0c * g.T[1] * g.n[2], &X2));
+  TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)P0 * g.n[1] * g.n[2], &X1));
+  TRY(workspace(P, 2, sizeof(cx<T>) * (size_t)P0 * g.T[1] * g.n[2], &X2));
   const long long rows = (long long)g.n[1] * g.n[2];
-  const long long in1 = (long long)T0c * g.T[1];
-  TRY((run_real_pass<T, true>(P, "mv_r2c_d0", g.T[0], T0c, rows, fl, arr_store<cx<T>>(P, X1, 1, 0, T0c),
-                              (double)rows * (g.n[0] * sizeof(S) + T0c * e))));
-  TRY((run_pass<T, false>(P, "mv_c2c_d1", g.T[1], g.T[1], T0c, g.n[2], -1, -1,
-                          arr_load<cx<T>>(P, X1, T0c, (long long)T0c * g.n[1], 1, g.n[1]), NoMid(),
-                          arr_store<cx<T>>(P, X2, T0c, in1, 1), (double)T0c * g.n[2] * (g.n[1] + g.T[1]) * e)));
-  TRY((run_pass<T, false>(P, "mv_fused_d2", g.T[2], g.n[2], in1, 1, -1, +1, arr_load<cx<T>>(P, X2, in1, 0, 1, g.n[2]),
-                          mid, arr_store<cx<T>>(P, X2, in1, 0, 1), (double)in1 * (2.0 * g.n[2] * e + g.T[2] * lb))));
-  TRY((run_pass<T, false>(P, "mv_c2c_d1i", g.T[1], g.n[1], T0c, g.n[2], +1, +1,
-                          arr_load<cx<T>>(P, X2, T0c, in1, 1, g.T[1]), NoMid(),
-                          arr_store<cx<T>>(P, X1, T0c, (long long)T0c * g.n[1], 1),
-                          (double)T0c * g.n[2] * (g.n[1] + g.T[1]) * e)));
-  return run_real_pass<T, false>(P, "mv_c2r_d0", g.T[0], g.n[0], rows, arr_load<cx<T>>(P, X1, 1, 0, T0c, T0c), fs,
-                                 (double)rows * (T0c * e + g.n[0] * sizeof(S)));
+  const long long s2 = (long long)P0 * g.T[1];
+  TRY((run_freal<T, true>(P, "mv_r2c_d0", g.T[0], T0c, rows, fl, arr_store<cx<T>>(P, X1, 1, 0, P0),
+                          (double)rows * (g.n[0] * sizeof(S) + T0c * e))));
+  TRY((run_fpass<T, -1, -1, false, false>(P, "mv_c2c_d1", g.T[1], g.T[1], T0c, g.n[2],
+                                          arr_load<cx<T>>(P, X1, P0, (long long)P0 * g.n[1], 1, g.n[1]), NoMid(),
+                                          arr_store<cx<T>>(P, X2, P0, s2, 1),
+                                          (double)T0c * g.n[2] * (g.n[1] + g.T[1]) * e)));
+  // forward along dim 2, eigenvalue factor, backward along dim 2 (pencils k0 x k1)
+  TRY((run_fpass<T, -1, +1, false, false>(P, "mv_fused_d2", g.T[2], g.n[2], T0c, g.T[1],
+                                          arr_load<cx<T>>(P, X2, s2, P0, 1, g.n[2]), mid,
+                                          arr_store<cx<T>>(P, X2, s2, P0, 1),
+                                          (double)T0c * g.T[1] * (2.0 * g.n[2] * e + g.T[2] * lb))));
+  TRY((run_fpass<T, +1, +1, false, false>(P, "mv_c2c_d1i", g.T[1], g.n[1], T0c, g.n[2],
+                                          arr_load<cx<T>>(P, X2, P0, s2, 1, g.T[1]), NoMid(),
+                                          arr_store<cx<T>>(P, X1, P0, (long long)P0 * g.n[1], 1),
+                                          (double)T0c * g.n[2] * (g.n[1] + g.T[1]) * e)));
+  return run_freal<T, false>(P, "mv_c2r_d0", g.T[0], g.n[0], rows, arr_load<cx<T>>(P, X1, 1, 0, P0, T0c), fs,
+                             (double)rows * (T0c * e + g.n[0] * sizeof(S)));
 }
 
 // DFT field backend matvec: complex embedding, c2c on every axis, Re extraction
@@ -826,8 +934,9 @@ static pf_status matvec_dft(pf_plan* P, int op, const S* in, S* out) {
   TRY((run_pass<T, false>(P, "mv_dft_d1", g.T[1], g.T[1], g.T[0], g.n[2], -1, -1,
                           arr_load<cx<T>>(P, X1, g.T[0], (long long)g.T[0] * g.n[1], 1, g.n[1]), NoMid(),
                           arr_store<cx<T>>(P, X2, g.T[0], in1, 1), (double)g.T[0] * g.n[2] * (g.n[1] + g.T[1]) * e)));
-  TRY((run_pass<T, false>(P, "mv_dft_fused_d2", g.T[2], g.n[2], in1, 1, -1, +1, arr_load<cx<T>>(P, X2, in1, 0, 1, g.n[2]),
-                          mid, arr_store<cx<T>>(P, X2, in1, 0, 1), (double)in1 * 2.0 * g.n[2] * e)));
+  TRY((run_pass<T, false>(P, "mv_dft_fused_d2", g.T[2], g.n[2], g.T[0], g.T[1], -1, +1,
+                          arr_load<cx<T>>(P, X2, in1, g.T[0], 1, g.n[2]), mid, arr_store<cx<T>>(P, X2, in1, g.T[0], 1),
+                          (double)in1 * 2.0 * g.n[2] * e)));
   TRY((run_pass<T, false>(P, "mv_dft_d1i", g.T[1], g.n[1], g.T[0], g.n[2], +1, +1,
                           arr_load<cx<T>>(P, X2, g.T[0], in1, 1, g.T[1]), NoMid(),
                           arr_store<cx<T>>(P, X1, g.T[0], (long long)g.T[0] * g.n[1], 1),

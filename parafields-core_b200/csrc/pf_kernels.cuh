@@ -436,9 +436,23 @@ struct CovRowLoad {
 };
 
 // ---------------------------------------------------------------------------
-// counter-based normal noise: Philox2x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel
-// random numbers: as easy as 1, 2, 3", SC 2011) + Box-Muller
+// counter-based normal noise: Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel
+// random numbers: as easy as 1, 2, 3", SC 2011) + Box-Muller.  One call yields the
+// normals of two frequencies: k and k + T/2 along the last axis (the pair shares the
+// counter of its first member).  The 2x32 variant serves the DFT backend.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
 __device__ __forceinline__ uint2 philox2x32_10(uint2 ctr, uint32_t key) {
 #pragma unroll
   for (int r = 0; r < 10; r++) {
@@ -450,21 +464,33 @@ __device__ __forceinline__ uint2 philox2x32_10(uint2 ctr, uint32_t key) {
   return ctr;
 }
 
-__device__ __forceinline__ void sincospi_any(float x, float* s, float* c) { sincospif(x, s, c); }
-__device__ __forceinline__ void sincospi_any(double x, double* s, double* c) { sincospi(x, s, c); }
+// Box-Muller of two 32-bit words: u1 in (0,1), u2 in [0,1)
+__device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& r1, float& r2) {
+  const float u1 = ((float)a + 0.5f) * 2.3283064365386963e-10f;
+  const float rad = sqrtf(-1.3862943611198906f * __log2f(u1));  // -2 ln u1
+  float s, c;
+  __sincosf(6.283185307179586f * ((float)b * 2.3283064365386963e-10f) - 3.141592653589793f, &s, &c);
+  r1 = rad * c;
+  r2 = rad * s;
+}
+__device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, double& r1, double& r2) {
+  const double u1 = ((double)a + 0.5) * 2.3283064365386963e-10;
+  const double rad = sqrt(-2.0 * log(u1));
+  double s, c;
+  sincospi(2.0 * ((double)b * 2.3283064365386963e-10) - 1.0, &s, &c);
+  r1 = rad * c;
+  r2 = rad * s;
+}
+
+__device__ __forceinline__ uint4 pair_counter(uint64_t si) {
+  return make_uint4((uint32_t)si, (uint32_t)(si >> 32), 0x70616972u, 0u);
+}
 
 template <typename T>
 __device__ __forceinline__ void normal_pair(uint64_t seed, uint64_t idx, T& r1, T& r2) {
   const uint2 c = philox2x32_10(make_uint2((uint32_t)idx, (uint32_t)(idx >> 32) ^ (uint32_t)(seed >> 32)),
                                 (uint32_t)seed);
-  // u1 in (0, 1], u2 in [0, 1)
-  const T u1 = ((T)(c.x >> 8) + (T)1) * (T)(1.0 / 16777216.0);
-  const T u2 = (T)(c.y >> 8) * (T)(1.0 / 16777216.0);
-  const T rad = sqrt((T)-2 * log(u1));
-  T s, co;
-  sincospi_any(2 * u2, &s, &co);
-  r1 = rad * co;
-  r2 = rad * s;
+  box_muller(c.x, c.y, r1, r2);
 }
 
 // ---------------------------------------------------------------------------
@@ -482,42 +508,88 @@ struct R2CNoise {
   const double* noise;  // reference draw order, or null for the counter-based generator
   uint64_t seed;
   long long nsq, nnoise;  // buffer sizes (eigenvalues, noise doubles)
-  // pass geometry: the transform axis is dim-1 (first backward pass)
-  template <typename T>
-  __device__ __forceinline__ cx<T> load(long long p, int j, long long) const {
-    const int k0 = (int)(p % T0c);
-    const int k1 = dim == 3 ? (int)(p / T0c) : j;
-    const int k2 = dim == 3 ? j : 0;
-    // stored (reference) index of this frequency
-    uint64_t si;
-    if (transposed)
-      si = (uint64_t)k0 + (uint64_t)T0c * ((uint64_t)k2 + (uint64_t)ext[2] * (uint64_t)k1);
-    else
-      si = (uint64_t)k0 + (uint64_t)T0c * ((uint64_t)k1 + (uint64_t)ext[1] * (uint64_t)k2);
-    uint64_t li;
+  int Tl;                 // extended cells of the last dimension (the pass axis)
+  // The pass transforms along the last axis: p enumerates the other frequencies
+  // (k0 fastest), j is the last-axis frequency.
+  // pencils of the pass: k0 = p (fastest), k1 = the outer block index (3D)
+  __device__ __forceinline__ void decode(int p, int io, int& k0, int& k1) const {
+    k0 = p;
+    k1 = dim == 3 ? io : 0;
+  }
+  __device__ __forceinline__ uint64_t stored(int k0, int k1, int kl) const {
+    if (dim == 2) return (uint64_t)k0 + (uint64_t)T0c * (uint64_t)kl;
+    if (transposed) return (uint64_t)k0 + (uint64_t)T0c * ((uint64_t)kl + (uint64_t)ext[2] * (uint64_t)k1);
+    return (uint64_t)k0 + (uint64_t)T0c * ((uint64_t)k1 + (uint64_t)ext[1] * (uint64_t)kl);
+  }
+  __device__ __forceinline__ long long lam_index(int k0, int k1, int kl) const {
+    const int a1 = dim == 3 ? k1 : kl, a2 = dim == 3 ? kl : 0;
     if (dct == 1) {
-      const int m1 = k1 <= ext[1] / 2 ? k1 : ext[1] - k1;
-      const int m2 = k2 <= ext[2] / 2 ? k2 : ext[2] - k2;
-      li = (uint64_t)k0 + (uint64_t)D0 * ((uint64_t)m1 + (uint64_t)D1 * (uint64_t)m2);
-    } else if (dct == 2) {  // full DFT spectrum (dftmatrixbackend.hh:303-307)
-      li = (uint64_t)k0 + (uint64_t)ext[0] * ((uint64_t)k1 + (uint64_t)ext[1] * (uint64_t)k2);
-    } else {
-      li = (uint64_t)k0 + (uint64_t)T0c * ((uint64_t)k1 + (uint64_t)ext[1] * (uint64_t)k2);
+      const int m1 = a1 <= ext[1] / 2 ? a1 : ext[1] - a1;
+      const int m2 = a2 <= ext[2] / 2 ? a2 : ext[2] - a2;
+      return (long long)k0 + (long long)D0 * ((long long)m1 + (long long)D1 * m2);
     }
-    if (!in_bounds((long long)li, nsq)) return mk<T>(0, 0);
+    if (dct == 2)  // full DFT spectrum (dftmatrixbackend.hh:303-307)
+      return (long long)k0 + (long long)ext[0] * ((long long)a1 + (long long)ext[1] * a2);
+    return (long long)k0 + (long long)T0c * ((long long)a1 + (long long)ext[1] * a2);
+  }
+  template <typename T>
+  __device__ __forceinline__ cx<T> scale(int k0, int k1, int kl, T r1, T r2) const {
+    const long long li = lam_index(k0, k1, kl);
+    if (!in_bounds(li, nsq)) return mk<T>(0, 0);
     const T lam = ((const T*)sq)[li];
+    const int a1 = dim == 3 ? k1 : kl, a2 = dim == 3 ? kl : 0;
+    const bool selfconj = (k0 == 0 || 2 * k0 == ext[0]) && (a1 == 0 || 2 * a1 == ext[1]) &&
+                          (dim < 3 || a2 == 0 || 2 * a2 == ext[2]);
+    if (selfconj) return mk<T>(lam * r1, (T)0);
+    const T s = lam / (T)1.41421356237309504880168872420969808;
+    return mk<T>(s * r1, s * r2);
+  }
+  // reference draw order noise (parity mode) or the counter-based pair definition
+  template <typename T>
+  __device__ __forceinline__ cx<T> load(long long pl, int j, long long io) const {
+    int k0, k1;
+    decode((int)pl, (int)io, k0, k1);
+    const int L = Tl;
     T r1, r2;
     if (noise) {
+      const uint64_t si = stored(k0, k1, j);
       if (!in_bounds((long long)(2 * si + 1), nnoise)) return mk<T>(0, 0);
       r1 = (T)noise[2 * si];
       r2 = (T)noise[2 * si + 1];
     } else {
-      normal_pair<T>(seed, si, r1, r2);
+      const int h = L / 2;
+      const bool second = (L % 2 == 0) && j >= h;
+      const uint64_t si = stored(k0, k1, second ? j - h : j);
+      const uint4 c = philox4x32_10(pair_counter(si), make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+      if (second)
+        box_muller(c.z, c.w, r1, r2);
+      else
+        box_muller(c.x, c.y, r1, r2);
     }
-    const bool selfconj = ((2 * k0) % ext[0] == 0) && ((2 * k1) % ext[1] == 0) && (dim < 3 || (2 * k2) % ext[2] == 0);
-    if (selfconj) return mk<T>(lam * r1, (T)0);
-    const T s = lam / (T)1.41421356237309504880168872420969808;
-    return mk<T>(s * r1, s * r2);
+    return scale<T>(k0, k1, j, r1, r2);
+  }
+  // elements j and j + L/2 from one generator call (L even, no noise buffer)
+  template <typename T>
+  __device__ __forceinline__ void load2(int pl, int j, int io, cx<T>& v0, cx<T>& v1) const {
+    int k0, k1;
+    decode(pl, io, k0, k1);
+    const int h = Tl / 2;
+    T r1, r2, r3, r4;
+    if (noise) {
+      const uint64_t s0 = stored(k0, k1, j), s1 = stored(k0, k1, j + h);
+      if (!in_bounds((long long)(2 * s0 + 1), nnoise) || !in_bounds((long long)(2 * s1 + 1), nnoise)) return;
+      r1 = (T)noise[2 * s0];
+      r2 = (T)noise[2 * s0 + 1];
+      r3 = (T)noise[2 * s1];
+      r4 = (T)noise[2 * s1 + 1];
+    } else {
+      const uint4 c = philox4x32_10(pair_counter(stored(k0, k1, j)),
+                                    make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+      box_muller(c.x, c.y, r1, r2);
+      box_muller(c.z, c.w, r3, r4);
+    }
+    v0 = scale<T>(k0, k1, j, r1, r2);
+    v1 = scale<T>(k0, k1, j + h, r3, r4);
   }
 };
 
@@ -593,8 +665,9 @@ struct MultMid {
   int axis;      // axis of the fused pass (dim-1)
   const void* fac;  // factor per stored eigenvalue (precision of the pass)
   long long nfac;
+  // pencils: 1D one row; 2D k0 = p; 3D k0 = p, k1 = the outer block index
   template <typename T>
-  __device__ __forceinline__ cx<T> operator()(long long p, int j, long long, cx<T> v) const {
+  __device__ __forceinline__ cx<T> operator()(long long p, int j, long long io, cx<T> v) const {
     int k0, k1 = 0, k2 = 0;
     if (dim == 1) {
       k0 = j;
@@ -602,8 +675,8 @@ struct MultMid {
       k0 = (int)p;
       k1 = j;
     } else {
-      k0 = (int)(p % C0);
-      k1 = (int)(p / C0);
+      k0 = (int)p;
+      k1 = (int)io;
       k2 = j;
     }
     uint64_t li;

@@ -114,9 +114,10 @@ def test_cg_reference_mode(oracle, name):
     assert rel(x, xo) < 1e-8
     r_gpu = rel(oracle.matvec(d, lam, pfb200.OP_MUL, x), b)
     r_orc = rel(oracle.matvec(d, lam, pfb200.OP_MUL, xo), b)
-    # same algorithm, same quality: on the compactly supported cubic covariance the
-    # reference's 60 iterations stop far from convergence in both implementations
-    assert r_gpu <= 1.01 * r_orc + 1e-9
+    # same algorithm, same quality: either both stop far from convergence (the compactly
+    # supported cubic covariance within 60 iterations) or both stop on the stagnation rule
+    # once the residual is tiny (where the last FP64 bits decide the exact iteration)
+    assert r_gpu <= max(1.01 * r_orc, 1e-7)
     assert abs(rep["relative_residual"] - r_gpu) <= 1e-3 * r_gpu + 1e-14
 
 
