@@ -34,7 +34,7 @@ CONFIG = {"workload": "3d-matern32-axiparallel-256^3-factor2-fp32-realizations",
           "cells": [256, 256, 256], "torus": [512, 512, 512], "spectrum": "fp64 DCT-I (untimed, once)",
           "embedding.approximate": "true (the factor-2 embedding has 15269 eigenvalues below -1e-14, "
                                    "min -7.3e-8, which the reference clamps only with this key set)",
-          "noise": "counter-based Philox2x32-10 on device, seed per step",
+          "noise": "counter-based Philox4x32-10 on device (one call per frequency pair k, k+T/2), seed per step",
           "l2": "no flush: per-step traffic ~1 GB through intermediates of 269 MB and 135 MB (> 126 MB L2)"}
 
 

@@ -12,6 +12,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -391,9 +392,60 @@ static size_t cap_of(const pf_plan* P, const void* p) {
 
 // compile-time specialised passes for the common lengths; other lengths fall back to
 // the runtime-radix kernels above
+static int sm_count(pf_plan* P) {
+  static int cached[128] = {0};
+  const int d = P->device < 128 ? P->device : 0;
+  if (!cached[d]) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, P->device);
+    cached[d] = n > 0 ? n : 148;
+  }
+  return cached[d];
+}
+
+// persistent grid: resident CTAs per SM x SMs, at most one CTA per tile
+template <typename K>
+static pf_status persistent_grid(pf_plan* P, K kern, size_t smem, long long ntiles, unsigned* grid) {
+  int per = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kThreads, smem));
+  if (per < 1) per = 1;
+  long long g = (long long)per * sm_count(P);
+  if (g > ntiles) g = ntiles;
+  *grid = (unsigned)(g > 0 ? g : 1);
+  return PF_OK;
+}
+
+template <typename T, int SIGN, int SIGN2, class Mid, class St, int L>
+static pf_status launch_fpass_pipe(pf_plan* P, const char* name, int Lout, long long npencil, long long nouter,
+                                   ArrLoad<cx<T>> ld, Mid mid, St st, double bytes) {
+  constexpr int B = fast_B<T, L>();
+  PassArgs a{};
+  a.L = L;
+  a.Lout = Lout;
+  a.B = B;
+  a.npencil = npencil;
+  a.nouter = nouter;
+  const cx<T>* tw = nullptr;
+  TRY(twiddles<T>(P, L, &tw));
+  const size_t smem = (size_t)(3 * L * B + L) * sizeof(cx<T>);
+  auto kern = k_fpass_pipe<T, L, B, SIGN, SIGN2, Mid, St>;
+  TRY(set_smem(kern, smem));
+  const long long ntiles = (npencil + B - 1) / B * nouter;
+  if (ntiles <= 0) return PF_OK;
+  if (npencil > 0x7fffffffLL) return fail(PF_ERR_CONFIG, "pass %s too large", name);
+  unsigned grid = 1;
+  TRY(persistent_grid(P, kern, smem, ntiles, &grid));
+  ProfRec rec;
+  TRY(prof_begin(P, name, bytes, &rec));
+  kern<<<grid, kThreads, smem, P->stream>>>(a, tw, ld, mid, st);
+  return prof_end(P, &rec);
+}
+
 template <typename T, int SIGN, int SIGN2, bool CONTIG, bool PAIR, class Ld, class Mid, class St, int L>
 static pf_status launch_fpass(pf_plan* P, const char* name, int Lout, long long npencil, long long nouter, Ld ld,
                               Mid mid, St st, double bytes) {
+  if constexpr (!CONTIG && !PAIR && std::is_same<Ld, ArrLoad<cx<T>>>::value)
+    return launch_fpass_pipe<T, SIGN, SIGN2, Mid, St, L>(P, name, Lout, npencil, nouter, ld, mid, st, bytes);
   constexpr int B = fast_B<T, L>();
   PassArgs a{};
   a.L = L;
@@ -447,6 +499,20 @@ static pf_status launch_freal(pf_plan* P, const char* name, int Lout, long long 
   const cx<T>* twT = nullptr;
   TRY(twiddles<T>(P, L, &tw));
   TRY(twiddles<T>(P, 2 * L, &twT));
+  if constexpr (!R2C && std::is_same<Ld, ArrLoad<cx<T>>>::value) {
+    const size_t smemp = (size_t)(3 * (L + 1) * B + 2 * L) * sizeof(cx<T>);
+    auto kern = k_fc2r_pipe<T, L, B, St>;
+    TRY(set_smem(kern, smemp));
+    const long long ntiles = (rows + B - 1) / B;
+    if (ntiles <= 0) return PF_OK;
+    if (rows > 0x7fffffffLL) return fail(PF_ERR_CONFIG, "pass %s too large", name);
+    unsigned grid = 1;
+    TRY(persistent_grid(P, kern, smemp, ntiles, &grid));
+    ProfRec rec;
+    TRY(prof_begin(P, name, bytes, &rec));
+    kern<<<grid, kThreads, smemp, P->stream>>>(a, tw, twT, ld, st);
+    return prof_end(P, &rec);
+  }
   const size_t smem = (size_t)(2 * (L + 1) * B + 2 * L) * sizeof(cx<T>);
   const long long grid = (rows + B - 1) / B;
   if (grid <= 0) return PF_OK;

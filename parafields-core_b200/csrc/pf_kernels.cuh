@@ -541,7 +541,9 @@ struct R2CNoise {
     const bool selfconj = (k0 == 0 || 2 * k0 == ext[0]) && (a1 == 0 || 2 * a1 == ext[1]) &&
                           (dim < 3 || a2 == 0 || 2 * a2 == ext[2]);
     if (selfconj) return mk<T>(lam * r1, (T)0);
-    const T s = lam / (T)1.41421356237309504880168872420969808;
+    // FP64 keeps the reference's lambda / sqrt(2) (r2cfieldbackend.hh:322-323)
+    const T s = sizeof(T) == 8 ? lam / (T)1.41421356237309504880168872420969808
+                               : lam * (T)0.70710678118654752440084436210484903928;
     return mk<T>(s * r1, s * r2);
   }
   // reference draw order noise (parity mode) or the counter-based pair definition
