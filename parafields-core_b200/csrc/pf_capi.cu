@@ -427,7 +427,7 @@ static pf_status launch_fpass_pipe(pf_plan* P, const char* name, int Lout, long 
   a.nouter = nouter;
   const cx<T>* tw = nullptr;
   TRY(twiddles<T>(P, L, &tw));
-  const size_t smem = (size_t)(3 * L * B + L) * sizeof(cx<T>);
+  const size_t smem = fast_smem_pipe<T, L>();
   auto kern = k_fpass_pipe<T, L, B, SIGN, SIGN2, Mid, St>;
   TRY(set_smem(kern, smem));
   const long long ntiles = (npencil + B - 1) / B * nouter;
@@ -457,7 +457,7 @@ static pf_status launch_fpass(pf_plan* P, const char* name, int Lout, long long 
   a.sign2 = SIGN2;
   const cx<T>* tw = nullptr;
   TRY(twiddles<T>(P, L, &tw));
-  const size_t smem = (size_t)(2 * L * B + L) * sizeof(cx<T>);
+  const size_t smem = fast_smem_pass<T, L>();
   auto kern = k_fpass<T, L, B, SIGN, SIGN2, CONTIG, PAIR, Ld, Mid, St>;
   TRY(set_smem(kern, smem));
   const long long tiles = (npencil + B - 1) / B;
@@ -500,7 +500,7 @@ static pf_status launch_freal(pf_plan* P, const char* name, int Lout, long long 
   TRY(twiddles<T>(P, L, &tw));
   TRY(twiddles<T>(P, 2 * L, &twT));
   if constexpr (!R2C && std::is_same<Ld, ArrLoad<cx<T>>>::value) {
-    const size_t smemp = (size_t)(3 * (L + 1) * B + 2 * L) * sizeof(cx<T>);
+    const size_t smemp = fast_smem_real_pipe<T, L>();
     auto kern = k_fc2r_pipe<T, L, B, St>;
     TRY(set_smem(kern, smemp));
     const long long ntiles = (rows + B - 1) / B;
@@ -513,7 +513,7 @@ static pf_status launch_freal(pf_plan* P, const char* name, int Lout, long long 
     kern<<<grid, kThreads, smemp, P->stream>>>(a, tw, twT, ld, st);
     return prof_end(P, &rec);
   }
-  const size_t smem = (size_t)(2 * (L + 1) * B + 2 * L) * sizeof(cx<T>);
+  const size_t smem = fast_smem_real<T, L>();
   const long long grid = (rows + B - 1) / B;
   if (grid <= 0) return PF_OK;
   if (grid > 0x7fffffffLL || rows > 0x7fffffffLL) return fail(PF_ERR_CONFIG, "pass %s too large", name);
@@ -555,7 +555,7 @@ static ArrLoad<S> arr_load(const pf_plan* P, const void* p, long long jstride, l
                            int Lin) {
   ArrLoad<S> l;
   l.ptr = (const S*)p;
-  l.n = (long long)(cap_of(P, p) / sizeof(S));
+  l.n = (unsigned)std::min<size_t>(cap_of(P, p) / sizeof(S), 0xffffffffu);
   l.jstride = jstride;
   l.ostride = ostride;
   l.rowstride = rowstride;
@@ -567,7 +567,7 @@ template <typename S>
 static ArrStore<S> arr_store(const pf_plan* P, void* p, long long jstride, long long ostride, long long rowstride) {
   ArrStore<S> s;
   s.ptr = (S*)p;
-  s.n = (long long)(cap_of(P, p) / sizeof(S));
+  s.n = (unsigned)std::min<size_t>(cap_of(P, p) / sizeof(S), 0xffffffffu);
   s.jstride = jstride;
   s.ostride = ostride;
   s.rowstride = rowstride;
@@ -816,7 +816,7 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
   nz.nsq = (long long)g.S;
   nz.nnoise = (long long)g.noise;
   nz.Tl = g.T[g.dim - 1];
-  FieldRowStore<S> fs{out, g.n[0], transform, P->desc.boxcox_lambda, (long long)g.domain};
+  FieldRowStore<S> fs{out, g.n[0], transform, P->desc.boxcox_lambda, (unsigned)g.domain};
   const double e = sizeof(cx<T>);
   const double noise_b = noise_dev ? 16.0 : 0.0;
   const double lam_b = sizeof(T);
@@ -872,7 +872,7 @@ static pf_status gen_dft(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
   nz.seed = seed;
   nz.nsq = (long long)g.S;
   nz.nnoise = (long long)g.noise;
-  SplitStore<S> ss{out, spare, g.n[0], transform, P->desc.boxcox_lambda, (long long)g.domain};
+  SplitStore<S> ss{out, spare, g.n[0], transform, P->desc.boxcox_lambda, (unsigned)g.domain};
   const double e = sizeof(cx<T>);
   if (g.dim == 1) {
     return run_pass<T, true>(P, "gen_dft_d0", g.T[0], g.n[0], 1, 1, +1, +1, nz, NoMid(), ss,
@@ -928,8 +928,8 @@ static pf_status matvec_r2c(pf_plan* P, int op, const S* in, S* out) {
   const int T0c = g.T0c, P0 = half_pitch(g);
   const double e = sizeof(cx<T>);
   const double lb = sizeof(T);
-  FieldRowLoad<S> fl{in, g.n[0], (long long)g.domain};
-  FieldRowStore<S> fs{out, g.n[0], 0, 0.0, (long long)g.domain};
+  FieldRowLoad<S> fl{in, g.n[0], (unsigned)g.domain};
+  FieldRowStore<S> fs{out, g.n[0], 0, 0.0, (unsigned)g.domain};
   if (g.dim == 2) {
     void* X1 = nullptr;
     TRY(workspace(P, 2, sizeof(cx<T>) * (size_t)P0 * g.n[1], &X1));
@@ -974,8 +974,8 @@ static pf_status matvec_dft(pf_plan* P, int op, const S* in, S* out) {
   TRY(factor_array<T>(P, op, &fac));
   MultMid mid = mult_mid<T>(P, fac);
   const double e = sizeof(cx<T>);
-  FieldComplexLoad<S> fl{in, g.n[0], (long long)g.domain};
-  SplitStore<S> ss{out, nullptr, g.n[0], 0, 0.0, (long long)g.domain};
+  FieldComplexLoad<S> fl{in, g.n[0], (unsigned)g.domain};
+  SplitStore<S> ss{out, nullptr, g.n[0], 0, 0.0, (unsigned)g.domain};
   if (g.dim == 1)
     return run_pass<T, true>(P, "mv_dft_fused_d0", g.T[0], g.n[0], 1, 1, -1, +1, fl, mid, ss,
                              (double)g.T[0] * sizeof(T) + 2.0 * g.n[0] * sizeof(S));
@@ -1472,10 +1472,10 @@ extern "C" pf_status pf_matvec_static(pf_plan* P, int32_t op, const double* in, 
   k_static_twiddles<<<8, 256, 0, P->stream>>>(tw1, T1);
   P->launches += 3;
   CK(cudaGetLastError());
-  ArrStore<double2> xs{X, 1, 0, T0c, (long long)nX};
-  ArrLoad<double2> xl0{X, 1, 0, T0c, (long long)nX, T0c};
-  FieldRowLoad<double> fl{in, n0, (long long)g.domain};
-  FieldRowStore<double> fs{out, n0, 0, 0.0, (long long)g.domain};
+  ArrStore<double2> xs{X, 1u, 0u, (unsigned)T0c, (unsigned)nX};
+  ArrLoad<double2> xl0{X, 1u, 0u, (unsigned)T0c, (unsigned)nX, T0c};
+  FieldRowLoad<double> fl{in, n0, (unsigned)g.domain};
+  FieldRowStore<double> fs{out, n0, 0, 0.0, (unsigned)g.domain};
   // dimension 0 forward (r2c with zero padding)
   PassArgs a{};
   a.L = L0;
@@ -1507,8 +1507,8 @@ extern "C" pf_status pf_matvec_static(pf_plan* P, int32_t op, const double* in, 
   smem = smem_of(b, false, 16);
   if (smem > 227 * 1024) return fail(PF_ERR_CONFIG, "pencil of length %d does not fit in shared memory", T1);
   {
-    ArrLoad<double2> xl1{X, T0c, 0, 1, (long long)nX, n1};
-    ArrStore<double2> xs1{X, T0c, 0, 1, (long long)nX};
+    ArrLoad<double2> xl1{X, (unsigned)T0c, 0u, 1u, (unsigned)nX, n1};
+    ArrStore<double2> xs1{X, (unsigned)T0c, 0u, 1u, (unsigned)nX};
     auto kern = k_pass<double, false, ArrLoad<double2>, StaticMid, ArrStore<double2>>;
     TRY(set_smem(kern, smem));
     kern<<<(unsigned)((T0c + b.B - 1) / b.B), kThreads, smem, P->stream>>>(b, tw1, xl1, mid, xs1);

@@ -1,14 +1,18 @@
 // pf_fastfft.cuh -- compile-time specialised pencil passes for the common lengths.
 //
-// Same structure as k_pass / k_r2c / k_c2r (one HBM read and one HBM write per pass,
-// the whole 1D transform of B pencils in shared memory), but the length L, the tile
-// width B and the transform directions are template parameters: the radix schedule
-// (8, then 4 / 2, then 3 / 5 / 7) is unrolled at compile time, every index division
-// becomes a shift or a multiply, the twiddle table is staged once per CTA in shared
-// memory, and each thread keeps a fixed pencil b = threadIdx.x % B so the load/store
-// functors' per-pencil work is done once.  Shared layout: element (b, j) at j*B + b,
-// so B consecutive pencils of a strided axis (or B rows of a contiguous one) are read
-// and written as B-wide segments.
+// Same job as k_pass / k_r2c / k_c2r (one HBM read and one HBM write per pass, the
+// whole 1D transform of B pencils in shared memory), specialised for B200:
+//  - L, B and the directions are template parameters; the Stockham radix schedule
+//    (8, then 4 / 2, then 3 / 5 / 7) unrolls at compile time;
+//  - element (b, j) of a tile lives at row j + j/8 (one padding row every 8 rows) so
+//    the stride-8 stores of a radix-8 first stage hit distinct banks;
+//  - the first stage runs in registers on the values the loader (or the noise
+//    generator) produced, and the last stage writes its outputs straight to global
+//    memory, so a 3-stage transform touches shared memory 4 times per element;
+//  - each thread keeps one pencil b = threadIdx.x % B; B = 8 * threads / L, so every
+//    stage processes exactly one radix-8 butterfly column per thread;
+//  - passes over work arrays prefetch the next tile with cp.async (software
+//    pipelining across tiles in persistent CTAs).
 #pragma once
 
 #include "pf_kernels.cuh"
@@ -19,14 +23,41 @@ constexpr int pick_radix(int m) {
   return (m % 8 == 0) ? 8 : (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2 : (m % 3 == 0) ? 3 : (m % 5 == 0) ? 5 : (m % 7 == 0) ? 7 : m;
 }
 
-// pencils per tile: two buffers of L*B complex within PF_TILE_BYTES (default 32 KB)
-#ifndef PF_TILE_BYTES
-#define PF_TILE_BYTES 32768
-#endif
+// one radix-8 butterfly column per thread and stage: B = 8 * threads / L
 template <typename T, int L>
 constexpr int fast_B() {
-  constexpr int b = PF_TILE_BYTES / (2 * L * (int)sizeof(cx<T>));
-  return b >= 16 ? 16 : (b >= 8 ? 8 : (b >= 4 ? 4 : (b >= 2 ? 2 : 1)));
+  return (8 * kThreads / L) >= 16 ? 16 : ((8 * kThreads / L) >= 1 ? 8 * kThreads / L : 1);
+}
+
+// rows of one padded tile buffer holding `rows` logical rows
+constexpr int padded_rows(int rows) { return rows + rows / 8 + 1; }
+
+template <int B>
+__device__ __forceinline__ int sidx(int j, int b) {
+  return (j + (j >> 3)) * B + b;
+}
+
+// shared bytes of each kernel family (buffers + twiddle tables)
+template <typename T, int L>
+constexpr size_t fast_smem_pass() {
+  return (size_t)(2 * padded_rows(L) * fast_B<T, L>() + L) * sizeof(cx<T>);
+}
+template <typename T, int L>
+constexpr size_t fast_smem_pipe() {
+  return (size_t)(3 * padded_rows(L) * fast_B<T, L>() + L) * sizeof(cx<T>);
+}
+template <typename T, int L>
+constexpr size_t fast_smem_real() {
+  return (size_t)(2 * padded_rows(L + 1) * fast_B<T, L>() + 2 * L) * sizeof(cx<T>);
+}
+template <typename T, int L>
+constexpr size_t fast_smem_real_pipe() {
+  return (size_t)(3 * padded_rows(L + 1) * fast_B<T, L>() + 2 * L) * sizeof(cx<T>);
+}
+
+template <typename T>
+constexpr int fast_minblocks() {
+  return sizeof(T) == 4 ? 3 : 2;
 }
 
 template <typename T, int SIGN>
@@ -36,116 +67,153 @@ __device__ __forceinline__ cx<T> tw_s(const cx<T>* tw, int m) {
   return w;
 }
 
-// one radix-R butterfly column: V adjacent pencils share the index arithmetic and
-// the twiddle factors; for FP32 the V = 2 pencils move as one 128-bit access
-template <typename T, int V>
-struct PencilVec {
-  static __device__ __forceinline__ void ld(const cx<T>* p, cx<T>* v) {
+template <typename T, int R, int SIGN, int L>
+__device__ __forceinline__ void dft_r(cx<T>* v, const cx<T>* tw) {
+  if constexpr (R == 2 || R == 3 || R == 4 || R == 5 || R == 8) {
+    Dft<T, R>::run(v, SIGN, nullptr, L);
+  } else {  // generic odd prime radix from the shared twiddle table
+    cx<T> o[R];
 #pragma unroll
-    for (int i = 0; i < V; i++) v[i] = p[i];
-  }
-  static __device__ __forceinline__ void st(cx<T>* p, const cx<T>* v) {
+    for (int q = 0; q < R; q++) {
+      cx<T> s = v[0];
 #pragma unroll
-    for (int i = 0; i < V; i++) p[i] = v[i];
-  }
-};
-template <>
-struct PencilVec<float, 2> {
-  static __device__ __forceinline__ void ld(const float2* p, float2* v) {
-    const float4 q = *reinterpret_cast<const float4*>(p);
-    v[0] = make_float2(q.x, q.y);
-    v[1] = make_float2(q.z, q.w);
-  }
-  static __device__ __forceinline__ void st(float2* p, const float2* v) {
-    *reinterpret_cast<float4*>(p) = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
-  }
-};
-
-// pencils per butterfly column (2 = 128-bit shared accesses for FP32); 1 measured
-// faster on B200 (the wider column raises register use and lowers occupancy)
-template <typename T, int B>
-constexpr int fast_V() {
-  return 1;
-}
-
-template <typename T, int L, int B, int SIGN, int Ns>
-__device__ __forceinline__ void fstages(cx<T>*& src, cx<T>*& dst, const cx<T>* tw) {
-  if constexpr (Ns < L) {
-    constexpr int R = pick_radix(L / Ns);
-    constexpr int NBF = L / R;
-    constexpr int TWS = L / (Ns * R);
-    constexpr int V = fast_V<T, B>();
-    constexpr int BV = B / V;
-    constexpr int TSTEP = kThreads / BV;
-    const int bv = (threadIdx.x % BV) * V;
-    for (int t = threadIdx.x / BV; t < NBF; t += TSTEP) {
-      const int k = t % Ns;
-      cx<T> v[V][R];
-#pragma unroll
-      for (int r = 0; r < R; r++) {
-        cx<T> a[V];
-        PencilVec<T, V>::ld(src + (t + r * NBF) * B + bv, a);
-        if constexpr (Ns > 1) {
-          if (r > 0) {
-            const cx<T> w = tw_s<T, SIGN>(tw, r * k * TWS);
-#pragma unroll
-            for (int i = 0; i < V; i++) a[i] = cmul<T>(a[i], w);
-          }
-        }
-#pragma unroll
-        for (int i = 0; i < V; i++) v[i][r] = a[i];
-      }
-#pragma unroll
-      for (int i = 0; i < V; i++) {
-        if constexpr (R == 2 || R == 3 || R == 4 || R == 5 || R == 8) {
-          Dft<T, R>::run(v[i], SIGN, nullptr, L);
-        } else {
-          // generic odd prime radix from the shared twiddle table
-          cx<T> o[R];
-#pragma unroll
-          for (int q = 0; q < R; q++) {
-            cx<T> s = v[i][0];
-#pragma unroll
-            for (int r = 1; r < R; r++)
-              s = cadd<T>(s, cmul<T>(v[i][r], tw_s<T, SIGN>(tw, ((r * q) % R) * (L / R))));
-            o[q] = s;
-          }
-#pragma unroll
-          for (int q = 0; q < R; q++) v[i][q] = o[q];
-        }
-      }
-      const int base = (t / Ns) * Ns * R + k;
-#pragma unroll
-      for (int r = 0; r < R; r++) {
-        cx<T> a[V];
-#pragma unroll
-        for (int i = 0; i < V; i++) a[i] = v[i][r];
-        PencilVec<T, V>::st(dst + (base + r * Ns) * B + bv, a);
-      }
+      for (int r = 1; r < R; r++) s = cadd<T>(s, cmul<T>(v[r], tw_s<T, SIGN>(tw, ((r * q) % R) * (L / R))));
+      o[q] = s;
     }
-    __syncthreads();
-    cx<T>* tmp = src;
-    src = dst;
-    dst = tmp;
-    fstages<T, L, B, SIGN, Ns * R>(src, dst, tw);
+#pragma unroll
+    for (int q = 0; q < R; q++) v[q] = o[q];
   }
 }
 
-template <typename T>
-constexpr int fast_minblocks() {
-  return sizeof(T) == 4 ? 3 : 2;
+// Stockham stage Ns (smem -> smem).  Outputs of butterfly t go to base + r*Ns.
+template <typename T, int L, int B, int SIGN, int Ns>
+__device__ __forceinline__ void fstage(const cx<T>* src, cx<T>* dst, const cx<T>* tw) {
+  constexpr int R = pick_radix(L / Ns);
+  constexpr int NBF = L / R;
+  constexpr int TWS = L / (Ns * R);
+  constexpr int TSTEP = kThreads / B;
+  const int b = threadIdx.x % B;
+  for (int t = threadIdx.x / B; t < NBF; t += TSTEP) {
+    const int k = t % Ns;
+    cx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      cx<T> a = src[sidx<B>(t + r * NBF, b)];
+      if constexpr (Ns > 1) {
+        if (r > 0) a = cmul<T>(a, tw_s<T, SIGN>(tw, r * k * TWS));
+      }
+      v[r] = a;
+    }
+    dft_r<T, R, SIGN, L>(v, tw);
+    const int base = (t / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; r++) dst[sidx<B>(base + r * Ns, b)] = v[r];
+  }
 }
 
-// Complex pass.  Tile = B consecutive pencils (rows when CONTIG).  Optional fused
-// elementwise Mid between a SIGN and a SIGN2 transform.  Ld may provide
-// load2(p, j, io, v0, v1) producing elements j and j + L/2 together (PAIR).
+// last stage: outputs j = t + r*Ns go straight to out(j, value)
+template <typename T, int L, int B, int SIGN, int Ns, class Out>
+__device__ __forceinline__ void fstage_last(const cx<T>* src, const cx<T>* tw, const Out& out) {
+  constexpr int R = pick_radix(L / Ns);
+  static_assert(Ns * R == L, "not the last stage");
+  constexpr int NBF = L / R;
+  constexpr int TWS = L / (Ns * R);
+  constexpr int TSTEP = kThreads / B;
+  const int b = threadIdx.x % B;
+  for (int t = threadIdx.x / B; t < NBF; t += TSTEP) {
+    cx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      cx<T> a = src[sidx<B>(t + r * NBF, b)];
+      if constexpr (Ns > 1) {
+        if (r > 0) a = cmul<T>(a, tw_s<T, SIGN>(tw, r * t * TWS));
+      }
+      v[r] = a;
+    }
+    dft_r<T, R, SIGN, L>(v, tw);
+#pragma unroll
+    for (int r = 0; r < R; r++) out(t + r * Ns, v[r]);
+  }
+}
+
+// middle stages from Ns up to (excluding) the last one, ping-ponging src/dst
+template <typename T, int L, int B, int SIGN, int Ns>
+__device__ __forceinline__ void fstages_mid(cx<T>*& src, cx<T>*& dst, const cx<T>* tw) {
+  if constexpr (Ns * pick_radix(L / Ns) < L) {
+    fstage<T, L, B, SIGN, Ns>(src, dst, tw);
+    __syncthreads();
+    cx<T>* t = src;
+    src = dst;
+    dst = t;
+    fstages_mid<T, L, B, SIGN, Ns * pick_radix(L / Ns)>(src, dst, tw);
+  }
+}
+
+// Ns of the last stage
+template <int L, int Ns = 1>
+constexpr int last_ns() {
+  if constexpr (Ns * pick_radix(L / Ns) < L)
+    return last_ns<L, Ns * pick_radix(L / Ns)>();
+  else
+    return Ns;
+}
+
+// all stages smem -> smem (result in src)
+template <typename T, int L, int B, int SIGN>
+__device__ __forceinline__ void fstages_all(cx<T>*& src, cx<T>*& dst, const cx<T>* tw) {
+  fstages_mid<T, L, B, SIGN, 1>(src, dst, tw);
+  fstage<T, L, B, SIGN, last_ns<L>()>(src, dst, tw);
+  __syncthreads();
+  cx<T>* t = src;
+  src = dst;
+  dst = t;
+}
+
+// first stage (Ns = 1) on register values v[r] = element t + r*L/R1; result to dst
+template <typename T, int L, int B, int SIGN>
+__device__ __forceinline__ void fstage_first_regs(cx<T>* v, int t, cx<T>* dst, const cx<T>* tw) {
+  constexpr int R = pick_radix(L);
+  dft_r<T, R, SIGN, L>(v, tw);
+  const int b = threadIdx.x % B;
+#pragma unroll
+  for (int r = 0; r < R; r++) dst[sidx<B>(t * R + r, b)] = v[r];
+}
+
+// the stages after a register first stage (src holds its output), ending in global
+template <typename T, int L, int B, int SIGN, class Out>
+__device__ __forceinline__ void fstages_rest_store(cx<T>*& src, cx<T>*& dst, const cx<T>* tw, const Out& out) {
+  constexpr int R1 = pick_radix(L);
+  fstages_mid<T, L, B, SIGN, R1>(src, dst, tw);
+  fstage_last<T, L, B, SIGN, last_ns<L>()>(src, tw, out);
+}
+
+// the stages after a register first stage, ending in shared memory (result in src)
+template <typename T, int L, int B, int SIGN>
+__device__ __forceinline__ void fstages_rest_smem(cx<T>*& src, cx<T>*& dst, const cx<T>* tw) {
+  constexpr int R1 = pick_radix(L);
+  if constexpr (R1 < L) {
+    fstages_mid<T, L, B, SIGN, R1>(src, dst, tw);
+    fstage<T, L, B, SIGN, last_ns<L>()>(src, dst, tw);
+    __syncthreads();
+    cx<T>* t = src;
+    src = dst;
+    dst = t;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Complex pass with a functor loader.  Tile = B consecutive pencils (rows when
+// CONTIG).  Optional fused elementwise Mid between a SIGN and a SIGN2 transform.
+// PAIR loaders produce elements j and j + L/2 together (load2).
+// ---------------------------------------------------------------------------
 template <typename T, int L, int B, int SIGN, int SIGN2, bool CONTIG, bool PAIR, class Ld, class Mid, class St>
 __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
     k_fpass(const PassArgs a, const cx<T>* __restrict__ twg, Ld ld, Mid mid, St st) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PR = padded_rows(L);
   cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
-  cx<T>* b1 = b0 + L * B;
-  cx<T>* tw = b1 + L * B;
+  cx<T>* b1 = b0 + PR * B;
+  cx<T>* tw = b1 + PR * B;
   for (int i = threadIdx.x; i < L; i += kThreads) tw[i] = __ldg(twg + i);
   int p0, io;
   const int np = (int)a.npencil;
@@ -157,48 +225,59 @@ __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
     io = blockIdx.x / tpo;
     p0 = (blockIdx.x - io * tpo) * B;
   }
+  constexpr int R1 = pick_radix(L);
+  constexpr int NBF1 = L / R1;
   constexpr int TSTEP = kThreads / B;
   const int b = threadIdx.x % B;
-  const int jt = threadIdx.x / B;
   const int p = p0 + b;
   const bool live = p < np;
-  if constexpr (PAIR) {
+  __syncthreads();  // twiddles
+  for (int t = threadIdx.x / B; t < NBF1; t += TSTEP) {
+    cx<T> v[R1];
+    if constexpr (PAIR) {
+      static_assert(R1 % 2 == 0, "paired loads need an even first radix");
 #pragma unroll
-    for (int j = jt; j < L / 2; j += TSTEP) {
-      cx<T> v0 = mk<T>(0, 0), v1 = mk<T>(0, 0);
-      if (live) ld.template load2<T>(p, j, io, v0, v1);
-      b0[j * B + b] = v0;
-      b0[(j + L / 2) * B + b] = v1;
+      for (int r = 0; r < R1 / 2; r++) {
+        cx<T> x0 = mk<T>(0, 0), x1 = mk<T>(0, 0);
+        if (live) ld.template load2<T>(p, t + r * NBF1, io, x0, x1);
+        v[r] = x0;
+        v[r + R1 / 2] = x1;
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < R1; r++) v[r] = live ? ld.template load<T>(p, t + r * NBF1, io) : mk<T>(0, 0);
     }
-  } else {
-#pragma unroll
-    for (int j = jt; j < L; j += TSTEP) b0[j * B + b] = live ? ld.template load<T>(p, j, io) : mk<T>(0, 0);
+    fstage_first_regs<T, L, B, SIGN>(v, t, b0, tw);
   }
   __syncthreads();
   cx<T>* src = b0;
   cx<T>* dst = b1;
-  fstages<T, L, B, SIGN, 1>(src, dst, tw);
+  const int Lout = a.Lout;
+  auto out = [&](int j, cx<T> v) {
+    if (live && j < Lout) st.template store<T>(p, j, io, v);
+  };
   if constexpr (Mid::active) {
+    fstages_rest_smem<T, L, B, SIGN>(src, dst, tw);
     if (live)
-      for (int j = jt; j < L; j += TSTEP) src[j * B + b] = mid.template operator()<T>(p, j, io, src[j * B + b]);
+      for (int j = threadIdx.x / B; j < L; j += TSTEP)
+        src[sidx<B>(j, b)] = mid.template operator()<T>(p, j, io, src[sidx<B>(j, b)]);
     __syncthreads();
-    fstages<T, L, B, SIGN2, 1>(src, dst, tw);
-  }
-  if (live) {
-#pragma unroll 8
-    for (int j = jt; j < a.Lout; j += TSTEP) st.template store<T>(p, j, io, src[j * B + b]);
+    fstages_mid<T, L, B, SIGN2, 1>(src, dst, tw);
+    fstage_last<T, L, B, SIGN2, last_ns<L>()>(src, tw, out);
+  } else {
+    fstages_rest_store<T, L, B, SIGN>(src, dst, tw, out);
   }
 }
 
-// Real-data passes along contiguous rows of 2L reals (see k_r2c / k_c2r for the
-// half-length algorithm); shared: two (L+1)*B buffers, then tables tw (L) and twT (L).
+// Real-to-complex rows (2L reals -> L+1 complex, half-length algorithm of k_r2c).
 template <typename T, int L, int B, class Ld, class St>
 __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
     k_fr2c(const PassArgs a, const cx<T>* __restrict__ twg, const cx<T>* __restrict__ twTg, Ld ld, St st) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PR = padded_rows(L + 1);
   cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
-  cx<T>* b1 = b0 + (L + 1) * B;
-  cx<T>* tw = b1 + (L + 1) * B;
+  cx<T>* b1 = b0 + PR * B;
+  cx<T>* tw = b1 + PR * B;
   cx<T>* twT = tw + L;
   for (int i = threadIdx.x; i < L; i += kThreads) {
     tw[i] = __ldg(twg + i);
@@ -206,43 +285,47 @@ __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
   }
   const int np = (int)a.npencil;
   const int p0 = blockIdx.x * B;
+  constexpr int R1 = pick_radix(L);
+  constexpr int NBF1 = L / R1;
   constexpr int TSTEP = kThreads / B;
   const int b = threadIdx.x % B;
-  const int jt = threadIdx.x / B;
   const int p = p0 + b;
   const bool live = p < np;
+  __syncthreads();
+  for (int t = threadIdx.x / B; t < NBF1; t += TSTEP) {
+    cx<T> v[R1];
 #pragma unroll
-  for (int m = jt; m < L; m += TSTEP) {
-    cx<T> z = mk<T>(0, 0);
-    if (live) z = mk<T>(ld.template real<T>(p, 2 * m), ld.template real<T>(p, 2 * m + 1));
-    b0[m * B + b] = z;
+    for (int r = 0; r < R1; r++) {
+      const int m = t + r * NBF1;
+      v[r] = live ? mk<T>(ld.template real<T>(p, 2 * m), ld.template real<T>(p, 2 * m + 1)) : mk<T>(0, 0);
+    }
+    fstage_first_regs<T, L, B, -1>(v, t, b0, tw);
   }
   __syncthreads();
   cx<T>* src = b0;
   cx<T>* dst = b1;
-  fstages<T, L, B, -1, 1>(src, dst, tw);
-  cx<T>* X = dst;
-  for (int k = jt; k <= L; k += TSTEP) {
-    const cx<T> zk = src[(k == L ? 0 : k) * B + b];
-    const cx<T> zm = conjg<T>(src[(k == 0 ? 0 : L - k) * B + b]);
-    const cx<T> e = cscale<T>(cadd<T>(zk, zm), (T)0.5);
-    const cx<T> o = cscale<T>(csub<T>(zk, zm), (T)0.5);
-    const cx<T> oi = mk<T>(o.y, -o.x);
-    const cx<T> w = (k == L) ? mk<T>(-1, 0) : twT[k];
-    X[k * B + b] = cadd<T>(e, cmul<T>(oi, w));
-  }
-  __syncthreads();
+  fstages_rest_smem<T, L, B, -1>(src, dst, tw);
   if (live)
-    for (int k = jt; k < a.Lout; k += TSTEP) st.template store<T>(p, k, 0, X[k * B + b]);
+    for (int k = threadIdx.x / B; k <= L && k < a.Lout; k += TSTEP) {
+      const cx<T> zk = src[sidx<B>(k == L ? 0 : k, b)];
+      const cx<T> zm = conjg<T>(src[sidx<B>(k == 0 ? 0 : L - k, b)]);
+      const cx<T> e = cscale<T>(cadd<T>(zk, zm), (T)0.5);
+      const cx<T> o = cscale<T>(csub<T>(zk, zm), (T)0.5);
+      const cx<T> oi = mk<T>(o.y, -o.x);
+      const cx<T> w = (k == L) ? mk<T>(-1, 0) : twT[k];
+      st.template store<T>(p, k, 0, cadd<T>(e, cmul<T>(oi, w)));
+    }
 }
 
+// Complex-to-real rows with a functor loader (FFTW c2r semantics, see k_c2r).
 template <typename T, int L, int B, class Ld, class St>
 __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
     k_fc2r(const PassArgs a, const cx<T>* __restrict__ twg, const cx<T>* __restrict__ twTg, Ld ld, St st) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PR = padded_rows(L + 1);
   cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
-  cx<T>* b1 = b0 + (L + 1) * B;
-  cx<T>* tw = b1 + (L + 1) * B;
+  cx<T>* b1 = b0 + PR * B;
+  cx<T>* tw = b1 + PR * B;
   cx<T>* twT = tw + L;
   for (int i = threadIdx.x; i < L; i += kThreads) {
     tw[i] = __ldg(twg + i);
@@ -252,33 +335,33 @@ __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
   const int p0 = blockIdx.x * B;
   constexpr int TSTEP = kThreads / B;
   const int b = threadIdx.x % B;
-  const int jt = threadIdx.x / B;
   const int p = p0 + b;
   const bool live = p < np;
-#pragma unroll
-  for (int k = jt; k <= L; k += TSTEP) {
+  for (int k = threadIdx.x / B; k <= L; k += TSTEP) {
     cx<T> v = live ? ld.template load<T>(p, k, 0) : mk<T>(0, 0);
     if (k == 0 || k == L) v.y = 0;
-    b1[k * B + b] = v;
+    b1[sidx<B>(k, b)] = v;
   }
   __syncthreads();
-  for (int k = jt; k < L; k += TSTEP) {
-    const cx<T> xk = b1[k * B + b];
-    const cx<T> xm = conjg<T>(b1[(L - k) * B + b]);
+  for (int k = threadIdx.x / B; k < L; k += TSTEP) {
+    const cx<T> xk = b1[sidx<B>(k, b)];
+    const cx<T> xm = conjg<T>(b1[sidx<B>(L - k, b)]);
     const cx<T> s = cadd<T>(xk, xm);
     const cx<T> d = csub<T>(xk, xm);
     const cx<T> t = cmul<T>(d, conjg<T>(twT[k]));
-    b0[k * B + b] = mk<T>(s.x - t.y, s.y + t.x);
+    b0[sidx<B>(k, b)] = mk<T>(s.x - t.y, s.y + t.x);
   }
   __syncthreads();
   cx<T>* src = b0;
   cx<T>* dst = b1;
-  fstages<T, L, B, +1, 1>(src, dst, tw);
-  if (live)
-    for (int j = jt; j < a.Lout; j += TSTEP) {
-      const cx<T> v = src[(j >> 1) * B + b];
-      st.template real<T>(p, j, (j & 1) ? v.y : v.x);
-    }
+  const int Lout = a.Lout;
+  auto out = [&](int m, cx<T> v) {
+    if (!live) return;
+    if (2 * m < Lout) st.template real<T>(p, 2 * m, v.x);
+    if (2 * m + 1 < Lout) st.template real<T>(p, 2 * m + 1, v.y);
+  };
+  fstages_mid<T, L, B, +1, 1>(src, dst, tw);
+  fstage_last<T, L, B, +1, last_ns<L>()>(src, tw, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -300,8 +383,8 @@ __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_g
 // copies element (p, j, o) of an ArrLoad array into shared (zero outside Lin / np)
 template <typename T>
 __device__ __forceinline__ void tile_copy(const ArrLoad<cx<T>>& ld, cx<T>* dst, int p, int np, int j, int o) {
-  const long long i = (long long)p * ld.rowstride + (long long)j * ld.jstride + (long long)o * ld.ostride;
-  const bool ok = p < np && j < ld.Lin && in_bounds(i, ld.n);
+  const unsigned i = (unsigned)p * ld.rowstride + (unsigned)j * ld.jstride + (unsigned)o * ld.ostride;
+  const bool ok = p < np && j < ld.Lin && in_bounds32(i, ld.n);
   if (sizeof(cx<T>) == 16)
     cp_async16(dst, ok ? (const void*)(ld.ptr + i) : (const void*)ld.ptr, ok ? 16 : 0);
   else
@@ -313,10 +396,11 @@ template <typename T, int L, int B, int SIGN, int SIGN2, class Mid, class St>
 __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
     k_fpass_pipe(const PassArgs a, const cx<T>* __restrict__ twg, ArrLoad<cx<T>> ld, Mid mid, St st) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PR = padded_rows(L);
   cx<T>* in0 = reinterpret_cast<cx<T>*>(smem_raw);
-  cx<T>* in1 = in0 + L * B;
-  cx<T>* work = in1 + L * B;
-  cx<T>* tw = work + L * B;
+  cx<T>* in1 = in0 + PR * B;
+  cx<T>* work = in1 + PR * B;
+  cx<T>* tw = work + PR * B;
   for (int i = threadIdx.x; i < L; i += kThreads) tw[i] = __ldg(twg + i);
   const int np = (int)a.npencil;
   const int tpo = (np + B - 1) / B;
@@ -328,7 +412,7 @@ __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
   if (t < ntiles) {
     const int o = (int)(t / tpo), p = (int)(t - (long long)o * tpo) * B + b;
 #pragma unroll 4
-    for (int j = jt; j < L; j += TSTEP) tile_copy<T>(ld, in0 + j * B + b, p, np, j, o);
+    for (int j = jt; j < L; j += TSTEP) tile_copy<T>(ld, in0 + sidx<B>(j, b), p, np, j, o);
   }
   cp_async_commit();
   for (int it = 0; t < ntiles; it++, t += gridDim.x) {
@@ -338,25 +422,30 @@ __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
     if (tn < ntiles) {
       const int o = (int)(tn / tpo), p = (int)(tn - (long long)o * tpo) * B + b;
 #pragma unroll 4
-      for (int j = jt; j < L; j += TSTEP) tile_copy<T>(ld, nxt + j * B + b, p, np, j, o);
+      for (int j = jt; j < L; j += TSTEP) tile_copy<T>(ld, nxt + sidx<B>(j, b), p, np, j, o);
     }
     cp_async_commit();
     cp_async_wait1();
     __syncthreads();
     const int o = (int)(t / tpo);
     const int p = (int)(t - (long long)o * tpo) * B + b;
+    const bool live = p < np;
+    const int Lout = a.Lout;
+    auto out = [&](int j, cx<T> v) {
+      if (live && j < Lout) st.template store<T>(p, j, o, v);
+    };
     cx<T>* src = cur;
     cx<T>* dst = work;
-    fstages<T, L, B, SIGN, 1>(src, dst, tw);
     if constexpr (Mid::active) {
-      if (p < np)
-        for (int j = jt; j < L; j += TSTEP) src[j * B + b] = mid.template operator()<T>(p, j, o, src[j * B + b]);
+      fstages_all<T, L, B, SIGN>(src, dst, tw);
+      if (live)
+        for (int j = jt; j < L; j += TSTEP) src[sidx<B>(j, b)] = mid.template operator()<T>(p, j, o, src[sidx<B>(j, b)]);
       __syncthreads();
-      fstages<T, L, B, SIGN2, 1>(src, dst, tw);
-    }
-    if (p < np) {
-#pragma unroll 8
-      for (int j = jt; j < a.Lout; j += TSTEP) st.template store<T>(p, j, o, src[j * B + b]);
+      fstages_mid<T, L, B, SIGN2, 1>(src, dst, tw);
+      fstage_last<T, L, B, SIGN2, last_ns<L>()>(src, tw, out);
+    } else {
+      fstages_mid<T, L, B, SIGN, 1>(src, dst, tw);
+      fstage_last<T, L, B, SIGN, last_ns<L>()>(src, tw, out);
     }
     __syncthreads();
   }
@@ -368,11 +457,11 @@ __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
     k_fc2r_pipe(const PassArgs a, const cx<T>* __restrict__ twg, const cx<T>* __restrict__ twTg,
                 ArrLoad<cx<T>> ld, St st) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int LP = L + 1;
+  constexpr int PR = padded_rows(L + 1);
   cx<T>* in0 = reinterpret_cast<cx<T>*>(smem_raw);
-  cx<T>* in1 = in0 + LP * B;
-  cx<T>* work = in1 + LP * B;
-  cx<T>* tw = work + LP * B;
+  cx<T>* in1 = in0 + PR * B;
+  cx<T>* work = in1 + PR * B;
+  cx<T>* tw = work + PR * B;
   cx<T>* twT = tw + L;
   for (int i = threadIdx.x; i < L; i += kThreads) {
     tw[i] = __ldg(twg + i);
@@ -387,7 +476,7 @@ __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
   if (t < ntiles) {
     const int p = (int)t * B + b;
 #pragma unroll 4
-    for (int k = jt; k <= L; k += TSTEP) tile_copy<T>(ld, in0 + k * B + b, p, np, k, 0);
+    for (int k = jt; k <= L; k += TSTEP) tile_copy<T>(ld, in0 + sidx<B>(k, b), p, np, k, 0);
   }
   cp_async_commit();
   for (int it = 0; t < ntiles; it++, t += gridDim.x) {
@@ -397,15 +486,16 @@ __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
     if (tn < ntiles) {
       const int p = (int)tn * B + b;
 #pragma unroll 4
-      for (int k = jt; k <= L; k += TSTEP) tile_copy<T>(ld, nxt + k * B + b, p, np, k, 0);
+      for (int k = jt; k <= L; k += TSTEP) tile_copy<T>(ld, nxt + sidx<B>(k, b), p, np, k, 0);
     }
     cp_async_commit();
     cp_async_wait1();
     __syncthreads();
     const int p = (int)t * B + b;
+    const bool live = p < np;
     for (int k = jt; k < L; k += TSTEP) {
-      cx<T> xk = cur[k * B + b];
-      cx<T> xm = cur[(L - k) * B + b];
+      cx<T> xk = cur[sidx<B>(k, b)];
+      cx<T> xm = cur[sidx<B>(L - k, b)];
       if (k == 0) {
         xk.y = 0;
         xm.y = 0;
@@ -414,19 +504,19 @@ __global__ void __launch_bounds__(kThreads, fast_minblocks<T>())
       const cx<T> s = cadd<T>(xk, xm);
       const cx<T> d = csub<T>(xk, xm);
       const cx<T> tt = cmul<T>(d, conjg<T>(twT[k]));
-      work[k * B + b] = mk<T>(s.x - tt.y, s.y + tt.x);
+      work[sidx<B>(k, b)] = mk<T>(s.x - tt.y, s.y + tt.x);
     }
     __syncthreads();
+    const int Lout = a.Lout;
+    auto out = [&](int m, cx<T> v) {
+      if (!live) return;
+      if (2 * m < Lout) st.template real<T>(p, 2 * m, v.x);
+      if (2 * m + 1 < Lout) st.template real<T>(p, 2 * m + 1, v.y);
+    };
     cx<T>* src = work;
     cx<T>* dst = cur;
-    fstages<T, L, B, +1, 1>(src, dst, tw);
-    if (p < np) {
-#pragma unroll 8
-      for (int j = jt; j < a.Lout; j += TSTEP) {
-        const cx<T> v = src[(j >> 1) * B + b];
-        st.template real<T>(p, j, (j & 1) ? v.y : v.x);
-      }
-    }
+    fstages_mid<T, L, B, +1, 1>(src, dst, tw);
+    fstage_last<T, L, B, +1, last_ns<L>()>(src, tw, out);
     __syncthreads();
   }
 }

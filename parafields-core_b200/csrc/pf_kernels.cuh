@@ -7,7 +7,10 @@
 
 namespace pf {
 
-constexpr int kThreads = 256;
+#ifndef PF_THREADS
+#define PF_THREADS 256
+#endif
+constexpr int kThreads = PF_THREADS;
 
 // Set by any functor whose computed index falls outside its buffer; the access is
 // skipped instead of performed, and the host turns the flag into an error.
@@ -15,6 +18,12 @@ __device__ unsigned int g_bounds_error;
 
 __device__ __forceinline__ bool in_bounds(long long i, long long n) {
   if (i >= 0 && i < n) return true;
+  atomicOr(&g_bounds_error, 1u);
+  return false;
+}
+// 32-bit element indices (every buffer of a plan holds fewer than 2^32 elements)
+__device__ __forceinline__ bool in_bounds32(unsigned i, unsigned n) {
+  if (i < n) return true;
   atomicOr(&g_bounds_error, 1u);
   return false;
 }
@@ -208,14 +217,14 @@ __global__ void __launch_bounds__(kThreads) k_c2r(const PassArgs a, const cx<T>*
 template <typename S>
 struct ArrLoad {
   const S* ptr;  // S = float2 or double2
-  long long jstride, ostride, rowstride;
-  long long n;  // elements in the buffer
-  int Lin;      // j >= Lin reads zero (input pruning / zero padding)
+  unsigned jstride, ostride, rowstride;
+  unsigned n;  // elements in the buffer
+  int Lin;     // j >= Lin reads zero (input pruning / zero padding)
   template <typename T>
   __device__ __forceinline__ cx<T> load(long long p, int j, long long o) const {
     if (j >= Lin) return mk<T>(0, 0);
-    const long long i = p * rowstride + j * jstride + o * ostride;
-    if (!in_bounds(i, n)) return mk<T>(0, 0);
+    const unsigned i = (unsigned)p * rowstride + (unsigned)j * jstride + (unsigned)o * ostride;
+    if (!in_bounds32(i, n)) return mk<T>(0, 0);
     const S v = ptr[i];
     return mk<T>((T)v.x, (T)v.y);
   }
@@ -224,12 +233,12 @@ struct ArrLoad {
 template <typename S>
 struct ArrStore {
   S* ptr;
-  long long jstride, ostride, rowstride;
-  long long n;
+  unsigned jstride, ostride, rowstride;
+  unsigned n;
   template <typename T>
   __device__ __forceinline__ void store(long long p, int j, long long o, cx<T> v) const {
-    const long long i = p * rowstride + j * jstride + o * ostride;
-    if (!in_bounds(i, n)) return;
+    const unsigned i = (unsigned)p * rowstride + (unsigned)j * jstride + (unsigned)o * ostride;
+    if (!in_bounds32(i, n)) return;
     S w;
     w.x = v.x;
     w.y = v.y;
@@ -257,12 +266,12 @@ template <typename S>
 struct FieldRowLoad {
   const S* x;
   int n0;
-  long long n;
+  unsigned n;
   template <typename T>
   __device__ __forceinline__ T real(long long p, int j) const {
     if (j >= n0) return (T)0;
-    const long long i = p * n0 + j;
-    return in_bounds(i, n) ? (T)x[i] : (T)0;
+    const unsigned i = (unsigned)p * (unsigned)n0 + (unsigned)j;
+    return in_bounds32(i, n) ? (T)x[i] : (T)0;
   }
 };
 
@@ -274,12 +283,12 @@ struct FieldRowStore {
   int n0;
   int transform;
   double boxcox;
-  long long n;
+  unsigned n;
   template <typename T>
   __device__ __forceinline__ void real(long long p, int j, T v) const {
     if (transform) v = apply_mutator<T>(transform, (T)boxcox, v);
-    const long long i = p * n0 + j;
-    if (in_bounds(i, n)) out[i] = (S)v;
+    const unsigned i = (unsigned)p * (unsigned)n0 + (unsigned)j;
+    if (in_bounds32(i, n)) out[i] = (S)v;
   }
 };
 
@@ -292,7 +301,7 @@ struct SplitStore {
   long long rowlen;
   int transform;
   double boxcox;
-  long long n;
+  unsigned n;
   template <typename T>
   __device__ __forceinline__ void store(long long p, int j, long long, cx<T> v) const {
     T a = v.x, b = v.y;
@@ -300,8 +309,8 @@ struct SplitStore {
       a = apply_mutator<T>(transform, (T)boxcox, a);
       b = apply_mutator<T>(transform, (T)boxcox, b);
     }
-    const long long i = p * rowlen + j;
-    if (!in_bounds(i, n)) return;
+    const unsigned i = (unsigned)p * (unsigned)rowlen + (unsigned)j;
+    if (!in_bounds32(i, n)) return;
     re[i] = (S)a;
     if (im) im[i] = (S)b;
   }
@@ -312,12 +321,12 @@ template <typename S>
 struct FieldComplexLoad {
   const S* x;
   int n0;
-  long long n;
+  unsigned n;
   template <typename T>
   __device__ __forceinline__ cx<T> load(long long p, int j, long long) const {
     if (j >= n0) return mk<T>(0, 0);
-    const long long i = p * n0 + j;
-    return mk<T>(in_bounds(i, n) ? (T)x[i] : (T)0, (T)0);
+    const unsigned i = (unsigned)p * (unsigned)n0 + (unsigned)j;
+    return mk<T>(in_bounds32(i, n) ? (T)x[i] : (T)0, (T)0);
   }
 };
 
@@ -486,6 +495,26 @@ __device__ __forceinline__ uint4 pair_counter(uint64_t si) {
   return make_uint4((uint32_t)si, (uint32_t)(si >> 32), 0x70616972u, 0u);
 }
 
+// SplitMix64 finaliser (Steele, Lea, Flood, "Fast splittable pseudorandom number
+// generators", OOPSLA 2014): the output function of the SplitMix64 sequence
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+// 128 random bits for the frequency pair whose first member has stored index si
+__device__ __forceinline__ uint4 pair_bits(uint64_t seed, uint64_t si) {
+#ifdef PF_NOISE_SPLITMIX
+  const uint64_t s = mix64(seed ^ 0x5851f42d4c957f2dull);
+  const uint64_t a = mix64(s + (2 * si) * 0x9e3779b97f4a7c15ull);
+  const uint64_t b = mix64(s + (2 * si + 1) * 0x9e3779b97f4a7c15ull);
+  return make_uint4((uint32_t)a, (uint32_t)(a >> 32), (uint32_t)b, (uint32_t)(b >> 32));
+#else
+  return philox4x32_10(pair_counter(si), make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+#endif
+}
+
 template <typename T>
 __device__ __forceinline__ void normal_pair(uint64_t seed, uint64_t idx, T& r1, T& r2) {
   const uint2 c = philox2x32_10(make_uint2((uint32_t)idx, (uint32_t)(idx >> 32) ^ (uint32_t)(seed >> 32)),
@@ -507,7 +536,7 @@ struct R2CNoise {
   const void* sq;     // sqrt(lambda), float or double per the pass precision
   const double* noise;  // reference draw order, or null for the counter-based generator
   uint64_t seed;
-  long long nsq, nnoise;  // buffer sizes (eigenvalues, noise doubles)
+  unsigned nsq, nnoise;   // buffer sizes (eigenvalues, noise doubles)
   int Tl;                 // extended cells of the last dimension (the pass axis)
   // The pass transforms along the last axis: p enumerates the other frequencies
   // (k0 fastest), j is the last-axis frequency.
@@ -516,26 +545,26 @@ struct R2CNoise {
     k0 = p;
     k1 = dim == 3 ? io : 0;
   }
-  __device__ __forceinline__ uint64_t stored(int k0, int k1, int kl) const {
-    if (dim == 2) return (uint64_t)k0 + (uint64_t)T0c * (uint64_t)kl;
-    if (transposed) return (uint64_t)k0 + (uint64_t)T0c * ((uint64_t)kl + (uint64_t)ext[2] * (uint64_t)k1);
-    return (uint64_t)k0 + (uint64_t)T0c * ((uint64_t)k1 + (uint64_t)ext[1] * (uint64_t)kl);
+  __device__ __forceinline__ unsigned stored(int k0, int k1, int kl) const {
+    if (dim == 2) return (unsigned)k0 + (unsigned)T0c * (unsigned)kl;
+    if (transposed) return (unsigned)k0 + (unsigned)T0c * ((unsigned)kl + (unsigned)ext[2] * (unsigned)k1);
+    return (unsigned)k0 + (unsigned)T0c * ((unsigned)k1 + (unsigned)ext[1] * (unsigned)kl);
   }
-  __device__ __forceinline__ long long lam_index(int k0, int k1, int kl) const {
+  __device__ __forceinline__ unsigned lam_index(int k0, int k1, int kl) const {
     const int a1 = dim == 3 ? k1 : kl, a2 = dim == 3 ? kl : 0;
     if (dct == 1) {
       const int m1 = a1 <= ext[1] / 2 ? a1 : ext[1] - a1;
       const int m2 = a2 <= ext[2] / 2 ? a2 : ext[2] - a2;
-      return (long long)k0 + (long long)D0 * ((long long)m1 + (long long)D1 * m2);
+      return (unsigned)k0 + (unsigned)D0 * ((unsigned)m1 + (unsigned)D1 * (unsigned)m2);
     }
     if (dct == 2)  // full DFT spectrum (dftmatrixbackend.hh:303-307)
-      return (long long)k0 + (long long)ext[0] * ((long long)a1 + (long long)ext[1] * a2);
-    return (long long)k0 + (long long)T0c * ((long long)a1 + (long long)ext[1] * a2);
+      return (unsigned)k0 + (unsigned)ext[0] * ((unsigned)a1 + (unsigned)ext[1] * (unsigned)a2);
+    return (unsigned)k0 + (unsigned)T0c * ((unsigned)a1 + (unsigned)ext[1] * (unsigned)a2);
   }
   template <typename T>
   __device__ __forceinline__ cx<T> scale(int k0, int k1, int kl, T r1, T r2) const {
-    const long long li = lam_index(k0, k1, kl);
-    if (!in_bounds(li, nsq)) return mk<T>(0, 0);
+    const unsigned li = lam_index(k0, k1, kl);
+    if (!in_bounds32(li, nsq)) return mk<T>(0, 0);
     const T lam = ((const T*)sq)[li];
     const int a1 = dim == 3 ? k1 : kl, a2 = dim == 3 ? kl : 0;
     const bool selfconj = (k0 == 0 || 2 * k0 == ext[0]) && (a1 == 0 || 2 * a1 == ext[1]) &&
@@ -554,15 +583,15 @@ struct R2CNoise {
     const int L = Tl;
     T r1, r2;
     if (noise) {
-      const uint64_t si = stored(k0, k1, j);
-      if (!in_bounds((long long)(2 * si + 1), nnoise)) return mk<T>(0, 0);
+      const unsigned si = stored(k0, k1, j);
+      if (!in_bounds32(2 * si + 1, nnoise)) return mk<T>(0, 0);
       r1 = (T)noise[2 * si];
       r2 = (T)noise[2 * si + 1];
     } else {
       const int h = L / 2;
       const bool second = (L % 2 == 0) && j >= h;
-      const uint64_t si = stored(k0, k1, second ? j - h : j);
-      const uint4 c = philox4x32_10(pair_counter(si), make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+      const unsigned si = stored(k0, k1, second ? j - h : j);
+      const uint4 c = pair_bits(seed, si);
       if (second)
         box_muller(c.z, c.w, r1, r2);
       else
@@ -578,15 +607,14 @@ struct R2CNoise {
     const int h = Tl / 2;
     T r1, r2, r3, r4;
     if (noise) {
-      const uint64_t s0 = stored(k0, k1, j), s1 = stored(k0, k1, j + h);
-      if (!in_bounds((long long)(2 * s0 + 1), nnoise) || !in_bounds((long long)(2 * s1 + 1), nnoise)) return;
+      const unsigned s0 = stored(k0, k1, j), s1 = stored(k0, k1, j + h);
+      if (!in_bounds32(2 * s0 + 1, nnoise) || !in_bounds32(2 * s1 + 1, nnoise)) return;
       r1 = (T)noise[2 * s0];
       r2 = (T)noise[2 * s0 + 1];
       r3 = (T)noise[2 * s1];
       r4 = (T)noise[2 * s1 + 1];
     } else {
-      const uint4 c = philox4x32_10(pair_counter(stored(k0, k1, j)),
-                                    make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+      const uint4 c = pair_bits(seed, stored(k0, k1, j));
       box_muller(c.x, c.y, r1, r2);
       box_muller(c.z, c.w, r3, r4);
     }
@@ -606,7 +634,7 @@ struct DFTNoise {
   const void* sq;
   const double* noise;
   uint64_t seed;
-  long long nsq, nnoise;
+  unsigned nsq, nnoise;
   template <typename T>
   __device__ __forceinline__ cx<T> load(long long p, int j, long long) const {
     int k[3] = {0, 0, 0};
@@ -640,11 +668,11 @@ struct DFTNoise {
     } else {
       li = (uint64_t)k[0] + (uint64_t)ext[0] * ((uint64_t)k[1] + (uint64_t)ext[1] * (uint64_t)k[2]);
     }
-    if (!in_bounds((long long)li, nsq)) return mk<T>(0, 0);
+    if (!in_bounds32((unsigned)li, nsq)) return mk<T>(0, 0);
     const T lam = ((const T*)sq)[li];
     T r1, r2;
     if (noise) {
-      if (!in_bounds((long long)(2 * si + 1), nnoise)) return mk<T>(0, 0);
+      if (!in_bounds32((unsigned)(2 * si + 1), nnoise)) return mk<T>(0, 0);
       r1 = (T)noise[2 * si];
       r2 = (T)noise[2 * si + 1];
     } else {
@@ -666,7 +694,7 @@ struct MultMid {
   int D0, D1;
   int axis;      // axis of the fused pass (dim-1)
   const void* fac;  // factor per stored eigenvalue (precision of the pass)
-  long long nfac;
+  unsigned nfac;
   // pencils: 1D one row; 2D k0 = p; 3D k0 = p, k1 = the outer block index
   template <typename T>
   __device__ __forceinline__ cx<T> operator()(long long p, int j, long long io, cx<T> v) const {
@@ -681,16 +709,16 @@ struct MultMid {
       k1 = (int)io;
       k2 = j;
     }
-    uint64_t li;
+    unsigned li;
     if (layout == 0) {
       const int m0 = k0 <= ext[0] / 2 ? k0 : ext[0] - k0;
       const int m1 = k1 <= ext[1] / 2 ? k1 : ext[1] - k1;
       const int m2 = k2 <= ext[2] / 2 ? k2 : ext[2] - k2;
-      li = (uint64_t)m0 + (uint64_t)D0 * ((uint64_t)m1 + (uint64_t)D1 * (uint64_t)m2);
+      li = (unsigned)m0 + (unsigned)D0 * ((unsigned)m1 + (unsigned)D1 * (unsigned)m2);
     } else {
-      li = (uint64_t)k0 + (uint64_t)LC0 * ((uint64_t)k1 + (uint64_t)ext[1] * (uint64_t)k2);
+      li = (unsigned)k0 + (unsigned)LC0 * ((unsigned)k1 + (unsigned)ext[1] * (unsigned)k2);
     }
-    if (!in_bounds((long long)li, nfac)) return mk<T>(0, 0);
+    if (!in_bounds32(li, nfac)) return mk<T>(0, 0);
     const T f = ((const T*)fac)[li];
     return mk<T>(v.x * f, v.y * f);
   }

@@ -1,0 +1,430 @@
+// randomfield.hh -- C++ mirror of parafields-core's RandomField / Matrix API for the
+// circulant-embedding path, running on the B200 library through the C ABI in
+// include/parafields_b200.h.
+//
+//   parafields_b200::ParameterTree config;   // same keys as Dune::ParameterTree configs
+//   config["grid.cells"] = "512 512"; ...
+//   parafields_b200::RandomField<2> field(config);
+//   field.generate(seed);                    // randomfield.hh:512-529
+//   field.timesMatrix();                     // randomfield.hh:1181-1202
+//
+// Noise: generate(seed) draws from std::default_random_engine + std::normal_distribution
+// in the reference's order (CppRNGBackend, backends/cpprngbackend.hh:16-59, used when GSL
+// is absent), so a reference build without GSL and this facade produce the same field
+// for the same seed up to floating-point rounding.  generateWithRNG accepts any object
+// with RF sample(), exactly like randomfield.hh:541-558.
+#pragma once
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <memory>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../../include/parafields_b200.h"
+#include "parametertree.hh"
+
+namespace parafields_b200 {
+
+// exceptions.hh:8-15
+class NegativeEigenvalueError : public std::runtime_error {
+ public:
+  explicit NegativeEigenvalueError(const std::string& what) : std::runtime_error(what) {}
+};
+
+inline void check(pf_status st) {
+  if (st == PF_OK) return;
+  const std::string msg = pf_last_error_string();
+  if (st == PF_ERR_NEG_EIGEN) throw NegativeEigenvalueError{msg};
+  throw std::runtime_error{msg};
+}
+
+// Configuration keys of the path -> descriptor (fieldtraits.hh:175-186, 229;
+// matrix.hh:232-260, 268-269, 479-493, 515-602; covariance.hh:33-128, 395-396, 515-516,
+// 711-713; mutators.hh:139-154).  Additional keys: gpu.precision (double|float, default
+// from RF) and gpu.eigenCheck (corrected|reference).
+template <unsigned dim, typename RF>
+pf_field_desc descFromConfig(const ParameterTree& config) {
+  pf_field_desc d;
+  pf_field_desc_init(&d);
+  d.dim = (int32_t)dim;
+  const auto cells = config.get<std::array<unsigned, dim>>("grid.cells");
+  const auto ext = config.get<std::array<double, dim>>("grid.extensions");
+  for (unsigned i = 0; i < dim; i++) {
+    d.cells[i] = (int32_t)cells[i];
+    d.extensions[i] = ext[i];
+  }
+  d.variance = config.get<double>("stochastic.variance");
+  const std::string cov = config.get<std::string>("stochastic.covariance");
+  static const char* names[] = {"exponential", "gaussian", "spherical", "separableExponential", "matern",
+                                "matern32", "matern52", "dampedOscillation", "gammaExponential", "cauchy",
+                                "generalizedCauchy", "cubic", "whiteNoise"};
+  d.covariance = -1;
+  for (int i = 0; i < 13; i++)
+    if (cov == names[i]) d.covariance = i;
+  if (d.covariance < 0 && cov != "custom-iso" && cov != "custom-aniso")
+    throw std::runtime_error{"covariance structure " + cov + " not known"};
+  if (d.covariance == PF_COV_MATERN) d.matern_nu = config.get<double>("stochastic.maternNu");
+  if (d.covariance == PF_COV_GAMMA_EXPONENTIAL) d.exp_gamma = config.get<double>("stochastic.expGamma");
+  if (d.covariance == PF_COV_GENERALIZED_CAUCHY) {
+    d.cauchy_alpha = config.get<double>("stochastic.cauchyAlpha");
+    d.cauchy_beta = config.get<double>("stochastic.cauchyBeta");
+  }
+  const std::string aniso = config.get<std::string>("stochastic.anisotropy", std::string("none"));
+  if (aniso == "none") {
+    d.anisotropy = PF_ANISO_NONE;
+    d.corr_length[0] = config.get<double>("stochastic.corrLength");
+  } else if (aniso == "axiparallel") {
+    d.anisotropy = PF_ANISO_AXIPARALLEL;
+    const auto c = config.get<std::array<double, dim>>("stochastic.corrLength");
+    for (unsigned i = 0; i < dim; i++) d.corr_length[i] = c[i];
+  } else if (aniso == "geometric") {
+    d.anisotropy = PF_ANISO_GEOMETRIC;
+    const auto c = config.get<std::array<double, dim * dim>>("stochastic.corrLength");
+    for (unsigned i = 0; i < dim * dim; i++) d.corr_length[i] = c[i];
+  } else {
+    throw std::runtime_error{"stochastic.anisotropy must be \"none\", \"axiparallel\" or \"geometric\""};
+  }
+  d.periodic = config.get<bool>("randomField.periodic", false);
+  d.approximate = config.get<bool>("embedding.approximate", false);
+  d.cg_iterations = (int32_t)config.get<unsigned>("randomField.cgIterations", 100u);
+  d.embedding_factor = (int32_t)config.get<unsigned>("embedding.factor", 2u);
+  d.threshold = config.get<double>("embedding.threshold", 1e-14);
+  if (config.hasKey("fftw.transposed")) d.transposed = config.get<bool>("fftw.transposed") ? 1 : 0;
+  const std::string per = config.get<std::string>("embedding.periodization", std::string("classical"));
+  if (per != "classical")
+    throw std::runtime_error{"embedding.periodization \"" + per + "\" is not available on the B200 path"};
+  const std::string optim = config.get<std::string>("embedding.optim", std::string("none"));
+  if (optim != "none") throw std::runtime_error{"optimization requires dune-nonlinopt"};
+  const std::string tr = config.get<std::string>("randomField.transform", std::string("none"));
+  if (tr == "none")
+    d.transform = PF_TRANSFORM_NONE;
+  else if (tr == "logNormal")
+    d.transform = PF_TRANSFORM_LOGNORMAL;
+  else if (tr == "foldedNormal")
+    d.transform = PF_TRANSFORM_FOLDEDNORMAL;
+  else if (tr == "sign")
+    d.transform = PF_TRANSFORM_SIGN;
+  else if (tr == "boxCox") {
+    d.transform = PF_TRANSFORM_BOXCOX;
+    d.boxcox_lambda = config.get<double>("transform.boxCoxLambda");
+  } else
+    throw std::runtime_error{"transform type not known"};
+  const std::string prec =
+      config.get<std::string>("gpu.precision", std::string(sizeof(RF) == 4 ? "float" : "double"));
+  d.precision = prec == "float" ? PF_PREC_F32 : PF_PREC_F64;
+  const std::string eig = config.get<std::string>("gpu.eigenCheck", std::string("corrected"));
+  d.eigen_check = eig == "reference" ? PF_EIGCHECK_REFERENCE : PF_EIGCHECK_CORRECTED;
+  return d;
+}
+
+// std::default_random_engine + std::normal_distribution (cpprngbackend.hh:16-59)
+template <typename RF>
+class CppRNGBackend {
+  std::default_random_engine generator;
+  std::normal_distribution<RF> normalDist{0., 1.};
+
+ public:
+  void seed(unsigned int s) { generator.seed(s); }
+  RF sample() { return normalDist(generator); }
+};
+
+// ValueTransform (mutators.hh:126-163)
+template <typename RF>
+class ValueTransform {
+  int kind = PF_TRANSFORM_NONE;
+  RF lambda = 0;
+
+ public:
+  ValueTransform() = default;
+  ValueTransform(int k, RF l) : kind(k), lambda(l) {}
+  void apply(RF& v) const {
+    switch (kind) {
+      case PF_TRANSFORM_LOGNORMAL: v = std::exp(v); break;
+      case PF_TRANSFORM_FOLDEDNORMAL: v = std::abs(v); break;
+      case PF_TRANSFORM_SIGN: v = v < 0. ? -1. : 1.; break;
+      case PF_TRANSFORM_BOXCOX: v = std::pow(v * lambda + 1, -lambda); break;
+      default: break;
+    }
+  }
+};
+
+// The Matrix of one field configuration (matrix.hh:55-206) on the GPU.
+template <typename RF>
+class GpuMatrix {
+  pf_plan* plan_ = nullptr;
+  pf_plan_info info_{};
+  pf_field_desc desc_{};
+  bool spare_pending_ = false;
+  bool custom_ = false;
+
+ public:
+  GpuMatrix(const pf_field_desc& d, bool customCovariance = false) : desc_(d), custom_(customCovariance) {
+    if ((d.precision == PF_PREC_F64) != (sizeof(RF) == 8))
+      throw std::runtime_error{"gpu.precision must match the field's value type"};
+    check(pf_plan_create(&d, &plan_));
+    check(pf_plan_get_info(plan_, &info_));
+  }
+  ~GpuMatrix() { pf_plan_destroy(plan_); }
+  GpuMatrix(const GpuMatrix&) = delete;
+  GpuMatrix& operator=(const GpuMatrix&) = delete;
+
+  const pf_plan_info& info() const { return info_; }
+  pf_plan* plan() const { return plan_; }
+
+  // fillTransformedMatrix(string) (matrix.hh:223-318)
+  pf_eig_stats fillTransformedMatrix() {
+    if (custom_) throw std::runtime_error{"you need to call fillMatrix with your covariance class as parameter"};
+    pf_eig_stats s{};
+    check(pf_spectrum_build(plan_, &s));
+    spare_pending_ = false;
+    return s;
+  }
+
+  // generateField (matrix.hh:330-421): the noise is drawn on the host in the reference's
+  // order, then scaled and transformed on the GPU; the DFT backend's second field is
+  // returned by the next call without drawing noise (matrix.hh:411-420)
+  template <typename RNG>
+  void generateField(RNG& rng, std::vector<RF>& data) {
+    data.resize(info_.domain_size);
+    std::vector<double> noise;
+    if (!spare_pending_) {
+      noise.resize(info_.noise_size);
+      for (auto& v : noise) v = (double)rng.sample();
+    }
+    check(pf_generate(plan_, noise.empty() ? nullptr : noise.data(), PF_MEM_HOST, 0, data.data(), PF_MEM_HOST, 0));
+    spare_pending_ = info_.field_backend == PF_FIELD_DFT && !spare_pending_;
+  }
+
+  // operator* / multiplyRoot / multiplyInverseExtended (matrix.hh:142-176, 1587-1646)
+  void multiply(int op, const std::vector<RF>& in, std::vector<RF>& out) const {
+    out.resize(in.size());
+    check(pf_matvec(plan_, op, sizeof(RF) == 8 ? PF_PREC_F64 : PF_PREC_F32, in.data(), out.data(), PF_MEM_HOST));
+  }
+
+  // multiplyInverse (matrix.hh:189-206); FP64 CG vectors
+  pf_cg_report multiplyInverse(const std::vector<RF>& in, std::vector<RF>& out, const pf_cg_opts* opts = nullptr) {
+    std::vector<double> b(in.begin(), in.end()), x(in.size());
+    pf_cg_report rep{};
+    pf_status st = pf_multiply_inverse(plan_, b.data(), x.data(), PF_MEM_HOST, opts, &rep);
+    if (st != PF_ERR_NOT_CONVERGED) check(st);
+    out.assign(x.begin(), x.end());
+    return rep;
+  }
+
+  // generateUncorrelatedField (matrix.hh:433-445): host white noise, seed + rank
+  void generateUncorrelatedField(unsigned int seed, std::vector<RF>& data) const {
+    std::default_random_engine generator(seed);
+    std::normal_distribution<RF> normalDist(0., 1.);
+    data.resize(info_.domain_size);
+    for (auto& v : data) v = normalDist(generator);
+  }
+
+  // setVarianceAsField (matrix.hh:456-462)
+  void setVarianceAsField(std::vector<RF>& data) const { data.assign(info_.domain_size, (RF)desc_.variance); }
+};
+
+// RandomField (randomfield.hh:42-1389) restricted to its stochastic part: the trend
+// part, file I/O and MPI redistribution are not part of this path.
+template <unsigned dim, typename RF = double>
+class RandomField {
+  ParameterTree config_;
+  pf_field_desc desc_;
+  ValueTransform<RF> transform_;
+  std::shared_ptr<GpuMatrix<RF>> matrix_;
+  std::vector<RF> data_;
+  bool cacheInvMatvec_, cacheInvRootMatvec_;
+  bool invMatvecValid_ = true, invRootMatvecValid_ = true;
+  std::vector<RF> invMatvecPart_, invRootMatvecPart_;
+  std::array<unsigned, dim> cells_;
+  std::array<double, dim> ext_;
+
+  void ensureMatrix() const {}
+
+ public:
+  explicit RandomField(const ParameterTree& config)
+      : config_(config),
+        desc_(descFromConfig<dim, RF>(config)),
+        cacheInvMatvec_(config.get<bool>("randomField.cacheInvMatvec", false)),
+        cacheInvRootMatvec_(config.get<bool>("randomField.cacheInvRootMatvec", false)) {
+    transform_ = ValueTransform<RF>(desc_.transform, (RF)desc_.boxcox_lambda);
+    const std::string cov = config.get<std::string>("stochastic.covariance");
+    matrix_ = std::make_shared<GpuMatrix<RF>>(desc_, cov == "custom-iso" || cov == "custom-aniso");
+    cells_ = config.get<std::array<unsigned, dim>>("grid.cells");
+    ext_ = config.get<std::array<double, dim>>("grid.extensions");
+    data_.assign(matrix_->info().domain_size, RF(0));
+    if (cacheInvMatvec_) invMatvecPart_ = data_;
+    if (cacheInvRootMatvec_) invRootMatvecPart_ = data_;
+  }
+
+  GpuMatrix<RF>& matrix() { return *matrix_; }
+  const std::vector<RF>& dataVector() const { return data_; }
+  std::vector<RF>& dataVector() { return data_; }
+
+  // randomfield.hh:512-529 (seed += rank; one rank here)
+  void generate(unsigned int seed) {
+    CppRNGBackend<RF> rng;
+    rng.seed(seed);
+    generateWithRNG(rng);
+  }
+
+  // randomfield.hh:541-558
+  template <typename RNG>
+  void generateWithRNG(RNG& rng) {
+    matrix_->generateField(rng, data_);
+    invMatvecValid_ = false;
+    invRootMatvecValid_ = false;
+  }
+
+  // randomfield.hh:593-612
+  void generateUncorrelated(unsigned int seed) {
+    matrix_->generateUncorrelatedField(seed, data_);
+    invMatvecValid_ = false;
+    invRootMatvecValid_ = false;
+  }
+
+  // randomfield.hh:641-651 with StochasticPart::evaluate (stochastic.hh:480-574) and
+  // coordsToIndices (fieldtraits.hh:443-451); a point on the upper boundary belongs to
+  // the last cell
+  void evaluate(const std::array<double, dim>& location, RF& output) const {
+    std::size_t index = 0, stride = 1;
+    for (unsigned i = 0; i < dim; i++) {
+      unsigned c = (unsigned)(location[i] * (cells_[i] + 1e-6) / ext_[i]);
+      if (c >= cells_[i]) c = cells_[i] - 1;
+      index += c * stride;
+      stride *= cells_[i];
+    }
+    output = data_[index];
+    transform_.apply(output);
+  }
+
+  // randomfield.hh:664-695
+  void bulkEvaluate(std::vector<RF>& output, std::array<unsigned, dim>& sizes) const {
+    sizes = cells_;
+    output = data_;
+    for (auto& v : output) transform_.apply(v);
+  }
+
+  // randomfield.hh:1181-1202
+  void timesMatrix() {
+    if (cacheInvMatvec_) {
+      invMatvecPart_ = data_;
+      invMatvecValid_ = true;
+    }
+    if (cacheInvRootMatvec_) {
+      matrix_->multiply(PF_OP_ROOT, data_, invRootMatvecPart_);
+      invRootMatvecValid_ = true;
+    }
+    std::vector<RF> out;
+    matrix_->multiply(PF_OP_MUL, data_, out);
+    data_.swap(out);
+  }
+
+  // randomfield.hh:1211-1238
+  void timesInverseMatrix() {
+    if (cacheInvMatvec_ && invMatvecValid_) {
+      if (cacheInvRootMatvec_) {
+        matrix_->multiply(PF_OP_ROOT, invMatvecPart_, invRootMatvecPart_);
+        invRootMatvecValid_ = true;
+      }
+      data_ = invMatvecPart_;
+      invMatvecValid_ = false;
+    } else {
+      std::vector<RF> out;
+      matrix_->multiplyInverse(data_, out);
+      data_.swap(out);
+      if (cacheInvMatvec_) invMatvecValid_ = false;
+      if (cacheInvRootMatvec_) invRootMatvecValid_ = false;
+    }
+  }
+
+  // randomfield.hh:1250-1268
+  void timesMatrixRoot() {
+    if (cacheInvMatvec_ && cacheInvRootMatvec_) {
+      invMatvecPart_ = invRootMatvecPart_;
+      invMatvecValid_ = invRootMatvecValid_;
+    }
+    if (cacheInvRootMatvec_) {
+      invRootMatvecPart_ = data_;
+      invRootMatvecValid_ = true;
+    }
+    std::vector<RF> out;
+    matrix_->multiply(PF_OP_ROOT, data_, out);
+    data_.swap(out);
+  }
+
+  // randomfield.hh:1278-1310
+  void timesInvMatRoot() {
+    if (cacheInvRootMatvec_ && invRootMatvecValid_) {
+      data_ = invRootMatvecPart_;
+      invRootMatvecValid_ = false;
+      if (cacheInvMatvec_) {
+        invRootMatvecPart_ = invMatvecPart_;
+        invRootMatvecValid_ = invMatvecValid_;
+        invMatvecValid_ = false;
+      }
+    } else {
+      std::vector<RF> out;
+      matrix_->multiplyInverse(data_, out);
+      data_.swap(out);
+      if (cacheInvRootMatvec_) {
+        invRootMatvecPart_ = data_;
+        invRootMatvecValid_ = true;
+      }
+      matrix_->multiply(PF_OP_ROOT, data_, out);
+      data_.swap(out);
+      if (cacheInvMatvec_) invMatvecValid_ = false;
+    }
+  }
+
+  // vector-space operations of the stochastic part (randomfield.hh:1027-1342)
+  RandomField& operator+=(const RandomField& o) {
+    for (std::size_t i = 0; i < data_.size(); i++) data_[i] += o.data_[i];
+    invMatvecValid_ = invRootMatvecValid_ = false;
+    return *this;
+  }
+  RandomField& operator-=(const RandomField& o) {
+    for (std::size_t i = 0; i < data_.size(); i++) data_[i] -= o.data_[i];
+    invMatvecValid_ = invRootMatvecValid_ = false;
+    return *this;
+  }
+  RandomField& operator*=(RF a) {
+    for (auto& v : data_) v *= a;
+    if (cacheInvMatvec_)
+      for (auto& v : invMatvecPart_) v *= a;
+    if (cacheInvRootMatvec_)
+      for (auto& v : invRootMatvecPart_) v *= a;
+    return *this;
+  }
+  RandomField& axpy(const RandomField& o, RF a) {
+    for (std::size_t i = 0; i < data_.size(); i++) data_[i] += a * o.data_[i];
+    invMatvecValid_ = invRootMatvecValid_ = false;
+    return *this;
+  }
+  RF operator*(const RandomField& o) const {
+    RF s = 0;
+    for (std::size_t i = 0; i < data_.size(); i++) s += data_[i] * o.data_[i];
+    return s;
+  }
+  RF oneNorm() const {
+    RF s = 0;
+    for (auto v : data_) s += std::abs(v);
+    return s;
+  }
+  RF twoNorm() const { return std::sqrt(*this * *this); }
+  RF infNorm() const {
+    RF m = 0;
+    for (auto v : data_) m = std::max(m, std::abs(v));
+    return m;
+  }
+  void zero() {
+    std::fill(data_.begin(), data_.end(), RF(0));
+    invMatvecValid_ = invRootMatvecValid_ = false;
+  }
+};
+
+}  // namespace parafields_b200

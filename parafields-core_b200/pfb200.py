@@ -16,7 +16,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libpfcuda.so")
+LIB_PATH = os.environ.get("PFB200_LIB", os.path.join(HERE, "lib", "libpfcuda.so"))
 
 # --- enums (include/parafields_b200.h) ---------------------------------------
 PF_OK, PF_ERR_NEG_EIGEN, PF_ERR_CONFIG, PF_ERR_OOM, PF_ERR_CUDA = 0, 1, 2, 3, 4

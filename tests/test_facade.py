@@ -1,0 +1,98 @@
+"""C++ facade (parafields-core_b200/include/parafields_b200/randomfield.hh): the
+reference's configuration keys and RandomField methods on top of the C ABI.
+CPU: key -> descriptor mapping and error messages.  GPU: generate(seed) with the
+reference's CppRNGBackend stream, timesMatrix, timesInverseMatrix against the oracle
+fed the same noise."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import pfb200
+from helpers import desc_of, rel
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def facade_exe(tmp_path_factory):
+    exe = tmp_path_factory.mktemp("facade") / "facade_main"
+    subprocess.run(["/usr/bin/g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "parafields-core_b200", "include"),
+                    "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp", "facade_main.cc"),
+                    "-o", str(exe), "-L", os.path.join(ROOT, "parafields-core_b200", "lib"), "-lpfcuda",
+                    "-Wl,-rpath," + os.path.join(ROOT, "parafields-core_b200", "lib")], check=True)
+    return str(exe)
+
+
+def write_ini(tmp_path, text):
+    p = tmp_path / "field.ini"
+    p.write_text(text)
+    return str(p)
+
+
+def test_config_keys(facade_exe, tmp_path):
+    ini = write_ini(tmp_path, """
+[grid]
+cells = 64 32
+extensions = 2 1
+[stochastic]
+variance = 1.5
+covariance = gammaExponential
+expGamma = 1.2
+anisotropy = geometric
+corrLength = 0.1 0.02 0.03 0.05
+[embedding]
+factor = 3
+approximate = true
+threshold = 1e-12
+[randomField]
+cgIterations = 50
+transform = boxCox
+[transform]
+boxCoxLambda = 0.25
+""")
+    out = subprocess.run([facade_exe, "config", ini], capture_output=True, text=True).stdout
+    assert "dim=2 cells=64,32,1 ext=2,1,1 factor=3 periodic=0 cov=8 var=1.5 aniso=2 corr=0.1,0.02,0.03,0.05" in out
+    assert "approx=1 thr=1e-12 transposed=-1 prec=0 eig=0 cg=50 transform=4 boxcox=0.25 gamma=1.2" in out
+
+
+@pytest.mark.parametrize("text,msg", [
+    ("grid.cells = 8 8\ngrid.extensions = 1 1\nstochastic.variance = 1\nstochastic.covariance = foo\n"
+     "stochastic.corrLength = 0.1\n", "covariance structure foo not known"),
+    ("grid.cells = 8 8\ngrid.extensions = 1 1\nstochastic.variance = 1\nstochastic.covariance = exponential\n"
+     "stochastic.corrLength = 0.1\nstochastic.anisotropy = weird\n", "stochastic.anisotropy must be"),
+    ("grid.cells = 8 8\ngrid.extensions = 1 1\nstochastic.variance = 1\nstochastic.covariance = exponential\n"
+     "stochastic.corrLength = 0.1\nrandomField.transform = cube\n", "transform type not known"),
+])
+def test_config_errors(facade_exe, tmp_path, text, msg):
+    out = subprocess.run([facade_exe, "config", write_ini(tmp_path, text)], capture_output=True, text=True).stdout
+    assert msg in out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim", [2, 3])
+def test_facade_generate_and_products(facade_exe, tmp_path, oracle, dim):
+    if dim == 2:
+        keys = "grid.cells = 48 40\ngrid.extensions = 1 1\nstochastic.corrLength = 0.1\n"
+        cfg = dict(dim=2, cells=(48, 40), covariance="exponential", corr_length=0.1)
+    else:
+        keys = "grid.cells = 16 12 10\ngrid.extensions = 1 1 1\nstochastic.anisotropy = axiparallel\n" \
+               "stochastic.corrLength = 0.1 0.08 0.05\n"
+        cfg = dict(dim=3, cells=(16, 12, 10), covariance="exponential", corr_length=(0.1, 0.08, 0.05))
+    ini = write_ini(tmp_path, keys + "stochastic.variance = 1\nstochastic.covariance = exponential\n"
+                    "randomField.transform = logNormal\nrandomField.cgIterations = 60\n")
+    r = subprocess.run([facade_exe, "run", ini, "17", str(tmp_path)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    ld = lambda n: np.fromfile(str(tmp_path / n), dtype=np.float64)
+    d = desc_of(cfg)
+    lam, _, _ = oracle.spectrum(d)
+    noise = ld("noise.bin")
+    field, _ = oracle.generate(d, lam, noise)
+    assert rel(ld("field.bin"), field) < 1e-11
+    assert rel(ld("bulk.bin"), np.exp(field)) < 1e-11
+    cx = oracle.matvec(d, lam, pfb200.OP_MUL, field)
+    assert rel(ld("cx.bin"), cx) < 1e-12
+    assert rel(ld("cinvcx.bin"), field) < 1e-6  # C^-1 (C x) = x up to the CG stopping rule
+    w = ld("white.bin")
+    assert abs(w.mean()) < 0.2 and abs(w.std() - 1) < 0.2
