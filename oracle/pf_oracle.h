@@ -50,6 +50,8 @@ int oc_resolve(const pf_field_desc* d, oc_geom* g, char* err, int errlen);
 
 /* One covariance functor (covariance.hh:296-823) at transformed coordinate x. */
 double oc_covariance(const pf_field_desc* d, const double* x);
+/* Modified Bessel function K_nu(x) (stands in for gsl_sf_bessel_Knu). */
+double oc_bessel_k(double nu, double x);
 /* Geometry transform (covariance.hh:18-138). */
 void oc_geometry(const pf_field_desc* d, const double* x, double* xt);
 

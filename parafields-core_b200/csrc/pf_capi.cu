@@ -131,7 +131,7 @@ static pf_status resolve(const pf_field_desc* d, Geom* g) {
   if (c < 0 || c > PF_COV_WHITE_NOISE) return fail(PF_ERR_CONFIG, "covariance structure not known");
   if (c == PF_COV_GAMMA_EXPONENTIAL && (d->exp_gamma < 0. || d->exp_gamma > 2.))
     return fail(PF_ERR_CONFIG, "exponent gamma has to be between 0 and 2");
-  if (c == PF_COV_MATERN) return fail(PF_ERR_CONFIG, "general matern requires the GNU Scientific Library (gsl)");
+  if (c == PF_COV_MATERN && d->matern_nu < 0.) return fail(PF_ERR_CONFIG, "matern nu has to be positive");
   if (c == PF_COV_GENERALIZED_CAUCHY) {
     if (d->cauchy_alpha <= 0. || d->cauchy_alpha > 2.)
       return fail(PF_ERR_CONFIG, "generalized Cauchy alpha has to be in range (0,2]");
@@ -631,6 +631,12 @@ static CovParams cov_params(const pf_field_desc* d, const Geom& g) {
   if (d->covariance == PF_COV_GENERALIZED_CAUCHY) {
     c.p0 = d->cauchy_alpha;
     c.p1 = d->cauchy_beta;
+  }
+  if (d->covariance == PF_COV_MATERN) {  // covariance.hh:515-520
+    c.p0 = std::sqrt(2. * d->matern_nu);
+    c.p1 = std::pow(2., 1. - d->matern_nu);
+    c.p2 = std::tgamma(d->matern_nu);
+    c.p3 = d->matern_nu;
   }
   return c;
 }

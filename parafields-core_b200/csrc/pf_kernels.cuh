@@ -344,8 +344,99 @@ struct CovParams {
   double wrap[3];   // ext * factor
   double geo[9];    // transformation applied to coordinates
   double variance;
-  double p0, p1;    // gamma / alpha / beta
+  double p0, p1;    // gamma / alpha / beta; matern: sqrt(2 nu), 2^(1-nu)
+  double p2, p3;    // matern: Gamma(nu), nu
 };
+
+// Modified Bessel function of the second kind K_nu(x), nu >= 0, x > 0.
+// Temme's series (N. M. Temme, J. Comput. Phys. 19, 324-337, 1975) for x <= 2 and
+// Steed's continued fraction CF2 (I. J. Thompson and A. R. Barnett, J. Comput. Phys.
+// 64, 490-509, 1986) for x > 2 give K_mu and K_mu+1 with |mu| <= 1/2; the upward
+// recurrence K_{m+1} = K_{m-1} + (2m/x) K_m reaches nu.  1/Gamma(1+z) enters through
+// its Taylor series (Abramowitz & Stegun 6.1.34; coefficients from the definition).
+__device__ __constant__ double RGAMMA_SERIES[24] = {1.0, 0.5772156649015328606065, -0.655878071520253881077, -0.042002635034095235529,
+    0.1665386113822914895017, -0.04219773455554433674821, -0.009621971527876973562115,
+    0.007218943246663099542395, -0.001165167591859065112114, -0.0002152416741149509728157,
+    0.0001280502823881161861532, -0.00002013485478078823865569, -0.000001250493482142670657345,
+    0.000001133027231981695882374, -2.05633841697760710345e-7, 6.116095104481415817862e-9,
+    5.002007644469222930056e-9, -1.181274570487020144588e-9, 1.043426711691100510492e-10,
+    7.78226343990507125405e-12, -3.696805618642205708188e-12, 5.100370287454475979015e-13,
+    -2.058326053566506783222e-14, -5.34812253942301798237e-15};
+
+__device__ inline double bessel_k(double nu, double x) {
+  const int nl = (int)(nu + 0.5);
+  const double mu = nu - nl, mu2 = mu * mu;
+  double kmu, kmu1;
+  if (x <= 2.0) {
+    const double x2 = 0.5 * x;
+    const double pimu = 3.14159265358979323846264338327950288 * mu;
+    const double fact = fabs(pimu) < 1e-15 ? 1.0 : pimu / sin(pimu);
+    const double d = -log(x2);
+    double e = mu * d;
+    const double fact2 = fabs(e) < 1e-15 ? 1.0 : sinh(e) / e;
+    double gam1 = 0.0, gam2 = 0.0, pw = 1.0;
+    for (int k = 0; k < 12; k++) {
+      gam2 += RGAMMA_SERIES[2 * k] * pw;
+      gam1 -= RGAMMA_SERIES[2 * k + 1] * pw;
+      pw *= mu2;
+    }
+    const double gampl = gam2 - mu * gam1; /* 1/Gamma(1+mu) */
+    const double gammi = gam2 + mu * gam1; /* 1/Gamma(1-mu) */
+    double ff = fact * (gam1 * cosh(e) + gam2 * fact2 * d);
+    double sum = ff;
+    e = exp(e);
+    double p = 0.5 * e / gampl;
+    double q = 0.5 / (e * gammi);
+    double c = 1.0;
+    const double dd = x2 * x2;
+    double sum1 = p;
+    for (int i = 1; i < 500; i++) {
+      ff = (i * ff + p + q) / (i * (double)i - mu2);
+      c *= dd / i;
+      p /= (i - mu);
+      q /= (i + mu);
+      const double del = c * ff;
+      sum += del;
+      sum1 += c * (p - i * ff);
+      if (fabs(del) < fabs(sum) * 1e-17) break;
+    }
+    kmu = sum;
+    kmu1 = sum1 * (2.0 / x);
+  } else {
+    double b = 2.0 * (1.0 + x);
+    double d = 1.0 / b;
+    double h = d, delh = d;
+    double q1 = 0.0, q2 = 1.0;
+    const double a1 = 0.25 - mu2;
+    double q = a1, c = a1, a = -a1;
+    double s = 1.0 + q * delh;
+    for (int i = 2; i < 100000; i++) {
+      a -= 2 * (i - 1);
+      c = -a * c / i;
+      const double qnew = (q1 - b * q2) / a;
+      q1 = q2;
+      q2 = qnew;
+      q += c * qnew;
+      b += 2.0;
+      d = 1.0 / (b + a * d);
+      delh = (b * d - 1.0) * delh;
+      h += delh;
+      const double dels = q * delh;
+      s += dels;
+      if (fabs(dels / s) < 1e-17) break;
+    }
+    h = a1 * h;
+    kmu = sqrt(3.14159265358979323846264338327950288 / (2.0 * x)) * exp(-x) / s;
+    kmu1 = kmu * (mu + x + 0.5 - h) / x;
+  }
+  double km = kmu, kp = kmu1;
+  for (int i = 1; i <= nl; i++) {
+    const double kn = km + (2.0 * (mu + i) / x) * kp;
+    km = kp;
+    kp = kn;
+  }
+  return km;
+}
 
 __device__ __forceinline__ double cov_eval(const CovParams& c, const double* xt) {
   const double var = c.variance;
@@ -397,6 +488,11 @@ __device__ __forceinline__ double cov_eval(const CovParams& c, const double* xt)
       const double h = sqrt(sum);
       if (h > 1.) return 0.;
       return var * (1. - 7. * pow(h, 2.) + 8.75 * pow(h, 3.) - 3.5 * pow(h, 5.) + 0.75 * pow(h, 7.));
+    }
+    case 4: {  // matern (covariance.hh:536-556), K_nu from bessel_k instead of GSL
+      const double h = sqrt(sum);
+      if (h < 1e-10) return var;
+      return var * c.p1 / c.p2 * pow(c.p0 * h, c.p3) * bessel_k(c.p3, c.p0 * h);
     }
     case 12:  // whiteNoise
       for (int i = 0; i < dim; i++)

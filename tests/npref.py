@@ -12,6 +12,7 @@ import numpy as np
 import scipy.fft as sf
 
 COV = {
+    "matern": 4,
     "exponential": 0, "gaussian": 1, "spherical": 2, "separableExponential": 3,
     "matern32": 5, "matern52": 6, "dampedOscillation": 7, "gammaExponential": 8,
     "cauchy": 9, "generalizedCauchy": 10, "cubic": 11, "whiteNoise": 12,
@@ -67,6 +68,13 @@ def covariance(cfg, xt):
         hh = np.minimum(h, 1.0)
         v = 1 - 7 * hh ** 2 + 8.75 * hh ** 3 - 3.5 * hh ** 5 + 0.75 * hh ** 7
         return np.where(h > 1, 0.0, var * v)
+    if c == "matern":
+        from scipy.special import gamma, kv
+        nu = cfg["matern_nu"]
+        z = np.sqrt(2 * nu) * h
+        with np.errstate(invalid="ignore"):
+            v = var * 2 ** (1 - nu) / gamma(nu) * z ** nu * kv(nu, np.where(z > 0, z, 1.0))
+        return np.where(h < 1e-10, var, v)
     if c == "whiteNoise":
         return np.where((np.abs(xt) > 1e-10).any(axis=-1), 0.0, var)
     raise ValueError(c)

@@ -33,6 +33,9 @@ CONFIGS = {
                        approximate=True),
     "3d-gexp-iso-notransp": dict(dim=3, cells=(16, 20, 24), covariance="gammaExponential", exp_gamma=1.3,
                                  corr_length=0.1, transposed=0),
+    "2d-matern-geo": dict(dim=2, cells=(40, 32), covariance="matern", matern_nu=1.7,
+                          corr_length=(0.1, 0.02, -0.01, 0.06), anisotropy="geometric", approximate=True),
+    "3d-matern-iso": dict(dim=3, cells=(20, 16, 12), covariance="matern", matern_nu=0.35, corr_length=0.1),
 }
 
 

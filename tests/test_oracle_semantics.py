@@ -13,6 +13,8 @@ CASES_2D = [
               "dampedOscillation", "cauchy", "cubic", "whiteNoise"]
 ] + [
     dict(dim=2, cells=(16, 12), covariance="gammaExponential", exp_gamma=1.5, corr_length=0.15),
+    dict(dim=2, cells=(16, 12), covariance="matern", matern_nu=0.8, corr_length=0.15),
+    dict(dim=2, cells=(16, 12), covariance="matern", matern_nu=2.7, corr_length=0.1, approximate=True),
     dict(dim=2, cells=(16, 12), covariance="generalizedCauchy", cauchy_alpha=1.2, cauchy_beta=2.0,
          corr_length=0.15),
     dict(dim=2, cells=(20, 14), covariance="exponential", corr_length=(0.2, 0.07), anisotropy="axiparallel",
@@ -24,6 +26,8 @@ CASES_3D = [
     dict(dim=3, cells=(8, 6, 10), covariance=c, corr_length=(0.2, 0.1, 0.15), anisotropy="axiparallel")
     for c in ["exponential", "matern32", "spherical", "gaussian"]
 ] + [
+    dict(dim=3, cells=(8, 6, 10), covariance="matern", matern_nu=1.3, corr_length=(0.2, 0.1, 0.15),
+         anisotropy="axiparallel", approximate=True),
     dict(dim=3, cells=(8, 6, 10), covariance="exponential",
          corr_length=(0.15, 0.02, 0.0, -0.03, 0.1, 0.01, 0.0, 0.02, 0.12), anisotropy="geometric",
          approximate=True),
@@ -149,7 +153,7 @@ def test_value_transforms(oracle, kind):
     (dict(dim=3, cells=(4, 4, 4), covariance="cubic", corr_length=0.1), "cubic"),
     (dict(covariance="gammaExponential", exp_gamma=2.5), "gamma"),
     (dict(covariance="generalizedCauchy", cauchy_alpha=3.0), "alpha"),
-    (dict(covariance="matern"), "gsl"),
+    (dict(covariance="matern", matern_nu=-1.0), "matern nu has to be positive"),
 ])
 def test_config_errors(oracle, over, msg):
     cfg = dict(dim=2, cells=(8, 8), covariance="exponential", corr_length=0.1)
@@ -166,3 +170,14 @@ def test_default_backends_and_layout(oracle):
     assert list(g.Ts) == [16, 8, 12]
     g = oracle.resolve(desc_of(dict(dim=1, cells=(32,), covariance="exponential", corr_length=0.1)))
     assert (g.matrix_backend, g.field_backend, g.transposed) == (pfb200.MATRIX_DFT, pfb200.FIELD_DFT, 0)
+
+
+@pytest.mark.parametrize("nu", [0.5, 1.5, 2.5])
+def test_general_matern_matches_closed_forms(oracle, nu):
+    """matern with nu = 1/2, 3/2, 5/2 equals exponential / matern32 / matern52 with the
+    correlation length scaled by sqrt(2 nu) (covariance.hh:502-625)."""
+    closed = {0.5: "exponential", 1.5: "matern32", 2.5: "matern52"}[nu]
+    ell = 0.12
+    a = desc_of(dict(dim=2, cells=(16, 12), covariance="matern", matern_nu=nu, corr_length=ell))
+    b = desc_of(dict(dim=2, cells=(16, 12), covariance=closed, corr_length=ell))
+    np.testing.assert_allclose(oracle.fill_matrix(a), oracle.fill_matrix(b), rtol=1e-12, atol=1e-15)
