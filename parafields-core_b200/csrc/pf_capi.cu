@@ -20,6 +20,7 @@
 #include "pf_cg.cuh"
 #include "pf_kernels.cuh"
 #include "pf_fastfft.cuh"
+#include "pf_pairfft.cuh"
 
 using namespace pf;
 
@@ -801,6 +802,8 @@ static pf_status factor_array(pf_plan* P, int op, const T** out) {
   return PF_OK;
 }
 
+#include "pf_pair_host.inc"
+
 // ---------------------------------------------------------------------------
 // generation: generateField (matrix.hh:330-421)
 // ---------------------------------------------------------------------------
@@ -839,7 +842,10 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
   const long long outer = g.dim == 3 ? g.T[1] : 1;
   const long long jst = g.dim == 3 ? (long long)P0 * g.T[1] : P0;
   const double b1 = (double)T0c * outer * (Tl * (noise_b + lam_b) + (double)g.n[last] * e);
-  if (Tl % 2 == 0)
+  constexpr bool F32 = std::is_same<T, float>::value && std::is_same<S, float>::value;
+  if (F32 && p2_length(Tl) && p2_view_ok(W1, jst, P0, outer))
+    TRY(p2_noise(P, "gen_noise_last", Tl, g.n[last], T0c, outer, nz, p2_store(P, W1, jst, P0, T0c), b1));
+  else if (Tl % 2 == 0)
     TRY((run_fpass<T, +1, +1, false, true>(P, "gen_noise_last", Tl, g.n[last], T0c, outer, nz, NoMid(),
                                            arr_store<cx<T>>(P, W1, jst, P0, 1), b1)));
   else
@@ -849,15 +855,42 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
   if (g.dim == 3) {
     void* W2 = nullptr;
     TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)P0 * g.n[1] * g.n[2], &W2));
-    TRY((run_fpass<T, +1, +1, false, false>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, g.n[2],
-                                            arr_load<cx<T>>(P, W1, P0, (long long)P0 * g.T[1], 1, g.T[1]),
-                                            NoMid(), arr_store<cx<T>>(P, W2, P0, (long long)P0 * g.n[1], 1),
-                                            (double)T0c * g.n[2] * (g.T[1] + g.n[1]) * e)));
+    const double b2 = (double)T0c * g.n[2] * (g.T[1] + g.n[1]) * e;
+    if (F32 && p2_length(g.T[1]) && p2_view_ok(W1, P0, (long long)P0 * g.T[1], g.n[2]) &&
+        p2_view_ok(W2, P0, (long long)P0 * g.n[1], g.n[2]))
+      TRY(p2_c2c<+1>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, g.n[2],
+                     p2_load(P, W1, P0, (long long)P0 * g.T[1], g.T[1], T0c),
+                     p2_store(P, W2, P0, (long long)P0 * g.n[1], T0c), b2));
+    else
+      TRY((run_fpass<T, +1, +1, false, false>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, g.n[2],
+                                              arr_load<cx<T>>(P, W1, P0, (long long)P0 * g.T[1], 1, g.T[1]),
+                                              NoMid(), arr_store<cx<T>>(P, W2, P0, (long long)P0 * g.n[1], 1),
+                                              b2)));
     cur = W2;
   }
   const long long rows = g.dim == 3 ? (long long)g.n[1] * g.n[2] : g.n[1];
-  return run_freal<T, false>(P, "gen_c2r_d0", g.T[0], g.n[0], rows, arr_load<cx<T>>(P, cur, 1, 0, P0, T0c), fs,
-                             (double)rows * (T0c * e + g.n[0] * sizeof(S)));
+  const double b3 = (double)rows * (T0c * e + g.n[0] * sizeof(S));
+  if constexpr (F32) {
+    if (g.T[0] % 2 == 0 && p2_length(g.T[0] / 2)) {
+      P2RowLoad rl;
+      rl.ptr = (const float2*)cur;
+      rl.rowstride = (unsigned)P0;
+      rl.n = (unsigned)std::min<size_t>(cap_of(P, cur) / sizeof(float2), 0xffffffffu);
+      rl.Lin = T0c;
+      rl.np = (int)rows;
+      P2FieldStore ps;
+      ps.out = (float*)out;
+      ps.n0 = g.n[0];
+      ps.transform = transform;
+      ps.boxcox = (float)P->desc.boxcox_lambda;
+      ps.n = (unsigned)g.domain;
+      ps.np = (int)rows;
+      ps.Lout = g.n[0];
+      ps.vec = (g.n[0] % 2 == 0 && ((uintptr_t)out & 7u) == 0) ? 1 : 0;
+      return p2_c2r(P, "gen_c2r_d0", g.T[0] / 2, g.n[0], rows, rl, ps, b3);
+    }
+  }
+  return run_freal<T, false>(P, "gen_c2r_d0", g.T[0], g.n[0], rows, arr_load<cx<T>>(P, cur, 1, 0, P0, T0c), fs, b3);
 }
 
 // DFT field backend: complex noise on the whole torus, backward c2c on every axis,

@@ -1,0 +1,509 @@
+// pf_pairfft.cuh -- FP32 pencil passes on Blackwell's paired FP32 instructions.
+//
+// Every thread transforms the same butterfly column of TWO pencils (A, B) at once.  The
+// pair's values live in "P2" form, re = (Re A, Re B) and im = (Im A, Im B), so each complex
+// add/subtract of a Stockham stage is one sm_100 FADD2/FFMA2 for both pencils and a
+// twiddle multiply is five (__fadd2_rn / __fmul2_rn / __ffma2_rn, PTX add/mul/fma.rn.f32x2):
+// half the issue slots of scalar butterflies, which is what bounds these passes.
+//
+// Layout and schedule (L a power of two, 64..2048, 256 threads, Q = 2048/L pairs per CTA):
+//  - a thread owns 8 P2 values of its pair; stage 1 (radix 8) runs on the values the
+//    loader produced, stages 2.. exchange through ONE padded shared buffer of 16-byte slots
+//    (Re A, Re B, Im A, Im B), slot(q, j) = q*PLQ + j + j/8, read-all / barrier / write-all;
+//  - the last stage writes its outputs straight to global memory (pruned to Lout);
+//  - per-stage twiddle tables are stored by (r-1)*Ns + k (k fastest), pre-broadcast as
+//    (wx, wx, wy, wy), so a warp's twiddle loads are conflict-free LDS.128;
+//  - CTAs are persistent: the tables are copied to shared memory once per CTA;
+//  - bounds violations are accumulated per thread and reported by one atomic at the end.
+#pragma once
+
+#include "pf_fastfft.cuh"
+
+namespace pf {
+
+constexpr int kP2Threads = 256;
+
+struct P2 {
+  float2 re, im;
+};
+
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+__device__ __forceinline__ P2 padd(const P2& a, const P2& b) { return {f2add(a.re, b.re), f2add(a.im, b.im)}; }
+__device__ __forceinline__ P2 psub(const P2& a, const P2& b) { return {f2sub(a.re, b.re), f2sub(a.im, b.im)}; }
+__device__ __forceinline__ P2 p2_of(float4 s) { return {make_float2(s.x, s.y), make_float2(s.z, s.w)}; }
+__device__ __forceinline__ float4 slot_of(const P2& a) { return make_float4(a.re.x, a.re.y, a.im.x, a.im.y); }
+// P2 from the complex values of pencil A and pencil B
+__device__ __forceinline__ P2 p2_ab(float2 a, float2 b) { return {make_float2(a.x, b.x), make_float2(a.y, b.y)}; }
+
+// a * w for a twiddle pre-broadcast as (wx, wx, wy, wy)
+__device__ __forceinline__ P2 ptw(const P2& a, float4 w) {
+  const float2 wx = make_float2(w.x, w.y), wy = make_float2(w.z, w.w);
+  return {f2sub(f2mul(a.re, wx), f2mul(a.im, wy)), f2fma(a.re, wy, f2mul(a.im, wx))};
+}
+
+// out[q] = sum_r v[r] exp(S 2 pi i r q / R), R = 2, 4, 8 (same conventions as Dft<T, R>)
+template <int S>
+__device__ __forceinline__ void pdft2(P2& v0, P2& v1) {
+  const P2 a = v0;
+  v0 = padd(a, v1);
+  v1 = psub(a, v1);
+}
+
+template <int S>
+__device__ __forceinline__ void pdft4(P2& v0, P2& v1, P2& v2, P2& v3) {
+  const P2 a = padd(v0, v2), b = psub(v0, v2), c = padd(v1, v3), d = psub(v1, v3);
+  v0 = padd(a, c);
+  v2 = psub(a, c);
+  if (S > 0) {  // X1 = b + i d, X3 = b - i d
+    v1 = {f2sub(b.re, d.im), f2add(b.im, d.re)};
+    v3 = {f2add(b.re, d.im), f2sub(b.im, d.re)};
+  } else {  // X1 = b - i d, X3 = b + i d
+    v1 = {f2add(b.re, d.im), f2sub(b.im, d.re)};
+    v3 = {f2sub(b.re, d.im), f2add(b.im, d.re)};
+  }
+}
+
+template <int S>
+__device__ __forceinline__ void pdft8(P2* v) {
+  P2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  P2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  pdft4<S>(e0, e1, e2, e3);
+  pdft4<S>(o0, o1, o2, o3);
+  const float2 h = make_float2(0.70710678118654752f, 0.70710678118654752f);
+  const float2 nh = make_float2(-0.70710678118654752f, -0.70710678118654752f);
+  v[0] = padd(e0, o0);
+  v[4] = psub(e0, o0);
+  // q = 2: o2 * (S i)
+  if (S > 0) {
+    v[2] = {f2sub(e2.re, o2.im), f2add(e2.im, o2.re)};
+    v[6] = {f2add(e2.re, o2.im), f2sub(e2.im, o2.re)};
+  } else {
+    v[2] = {f2add(e2.re, o2.im), f2sub(e2.im, o2.re)};
+    v[6] = {f2sub(e2.re, o2.im), f2add(e2.im, o2.re)};
+  }
+  // q = 1: o1 * W8 = h (o1.re - S o1.im, o1.im + S o1.re)
+  const float2 t1r = S > 0 ? f2sub(o1.re, o1.im) : f2add(o1.re, o1.im);
+  const float2 t1i = S > 0 ? f2add(o1.im, o1.re) : f2sub(o1.im, o1.re);
+  v[1] = {f2fma(h, t1r, e1.re), f2fma(h, t1i, e1.im)};
+  v[5] = {f2fma(nh, t1r, e1.re), f2fma(nh, t1i, e1.im)};
+  // q = 3: o3 * W8^3 = -h (o3.re + S o3.im, o3.im - S o3.re)
+  const float2 u = S > 0 ? f2add(o3.re, o3.im) : f2sub(o3.re, o3.im);
+  const float2 w = S > 0 ? f2sub(o3.im, o3.re) : f2add(o3.im, o3.re);
+  v[3] = {f2fma(nh, u, e3.re), f2fma(nh, w, e3.im)};
+  v[7] = {f2fma(h, u, e3.re), f2fma(h, w, e3.im)};
+}
+
+template <int R, int S>
+__device__ __forceinline__ void pdft(P2* v) {
+  if constexpr (R == 8) {
+    pdft8<S>(v);
+  } else if constexpr (R == 4) {
+    pdft4<S>(v[0], v[1], v[2], v[3]);
+  } else {
+    static_assert(R == 2, "power-of-two radices only");
+    pdft2<S>(v[0], v[1]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// compile-time geometry of a pair pass
+// ---------------------------------------------------------------------------
+template <int L>
+struct P2Geom {
+  static_assert(L >= 64 && L <= 2048 && (L & (L - 1)) == 0, "power-of-two length 64..2048");
+  static constexpr int TP = L / 8;                   // threads per pair
+  static constexpr int Q = kP2Threads / TP;          // pairs per CTA
+  static constexpr int NP = 2 * Q;                   // pencils per tile
+  // padded slots per pair: L + L/8 rounded so that the Q pairs of a warp phase fall in
+  // distinct 16-byte bank groups (residue 8/Q mod 8 for Q <= 8, odd beyond)
+  static constexpr int base = L + L / 8;
+  static constexpr int want = Q >= 8 ? 1 : (8 / Q) % 8;
+  static constexpr int PLQ = base + ((want - base % 8) + 8) % 8;
+  // twiddle entries of stages 2.. ((R-1) * Ns each)
+  template <int Ns = 8>
+  static constexpr int tw_entries() {
+    if constexpr (Ns >= L)
+      return 0;
+    else
+      return (pick_radix(L / Ns) - 1) * Ns + tw_entries<Ns * pick_radix(L / Ns)>();
+  }
+  static constexpr int NTW = tw_entries();
+};
+
+__device__ __forceinline__ int p2_slot(int PLQ, int q, int j) { return q * PLQ + j + (j >> 3); }
+
+// stages 2.. of the transform: v holds the thread's 8 values of stage Ns's input
+// (after stage 1 they are in buf).  Out(j, P2) receives the final outputs.
+template <int L, int S, int Ns, int TWOFF, class Out>
+__device__ __forceinline__ void p2_stages(P2 (&v)[8], float4* buf, const float4* tw, int u, int q,
+                                          const Out& out) {
+  using G = P2Geom<L>;
+  constexpr int R = pick_radix(L / Ns);
+  constexpr int NB = 8 / R;
+  constexpr int NBF = L / R;
+  constexpr bool LAST = Ns * R == L;
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < NB; i++) {
+    const int t = u + i * G::TP;
+#pragma unroll
+    for (int r = 0; r < R; r++) v[i * R + r] = p2_of(buf[p2_slot(G::PLQ, q, t + r * NBF)]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < NB; i++) {
+    const int t = u + i * G::TP;
+    const int k = t % Ns;
+#pragma unroll
+    for (int r = 1; r < R; r++) v[i * R + r] = ptw(v[i * R + r], tw[TWOFF + (r - 1) * Ns + k]);
+    pdft<R, S>(&v[i * R]);
+    if constexpr (LAST) {
+#pragma unroll
+      for (int r = 0; r < R; r++) out(t + r * Ns, v[i * R + r]);
+    } else {
+      const int base = (t / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; r++) buf[p2_slot(G::PLQ, q, base + r * Ns)] = slot_of(v[i * R + r]);
+    }
+  }
+  if constexpr (!LAST) p2_stages<L, S, Ns * R, TWOFF + (R - 1) * Ns>(v, buf, tw, u, q, out);
+}
+
+// whole transform from the stage-1 inputs v[r] = element u + r*L/8
+template <int L, int S, class Out>
+__device__ __forceinline__ void p2_transform(P2 (&v)[8], float4* buf, const float4* tw, int u, int q,
+                                             const Out& out) {
+  using G = P2Geom<L>;
+  pdft8<S>(v);
+#pragma unroll
+  for (int r = 0; r < 8; r++) buf[p2_slot(G::PLQ, q, u * 8 + r)] = slot_of(v[r]);
+  p2_stages<L, S, 8, 0>(v, buf, tw, u, q, out);
+}
+
+__device__ __forceinline__ void p2_copy_table(float4* dst, const float4* __restrict__ src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
+}
+
+__device__ __forceinline__ void p2_report(unsigned bad) {
+  if (bad) atomicOr(&g_bounds_error, 1u);
+}
+
+// ---------------------------------------------------------------------------
+// pair loaders / storers over the plan's arrays (element (p, j, o) at
+// p*rowstride + j*jstride + o*ostride, complex float)
+// ---------------------------------------------------------------------------
+// pencils p and p+1 adjacent (rowstride 1, even strides, 16-byte aligned base)
+struct P2ArrLoad {
+  const float4* ptr;  // pairs of complex
+  unsigned jstride, ostride;  // in complex elements (even)
+  unsigned n;                 // complex elements in the buffer
+  int Lin;
+  int np;
+  __device__ __forceinline__ P2 load(int p, int j, int o, unsigned& bad) const {
+    const unsigned i = (unsigned)p + (unsigned)j * jstride + (unsigned)o * ostride;
+    const bool want = j < Lin && p < np;
+    const bool ok = want && i + 1 < n;
+    bad |= (unsigned)(want && !ok);
+    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ok) s = ptr[i >> 1];
+    if (p + 1 >= np) {
+      s.z = 0.f;
+      s.w = 0.f;
+    }
+    return {make_float2(s.x, s.z), make_float2(s.y, s.w)};
+  }
+};
+
+struct P2ArrStore {
+  float4* ptr;
+  unsigned jstride, ostride;
+  unsigned n;
+  int np;
+  __device__ __forceinline__ void store(int p, int j, int o, const P2& v, unsigned& bad) const {
+    if (p >= np) return;
+    const unsigned i = (unsigned)p + (unsigned)j * jstride + (unsigned)o * ostride;
+    const bool two = p + 1 < np;
+    const bool ok = i + (two ? 1u : 0u) < n;
+    bad |= (unsigned)!ok;
+    if (!ok) return;
+    if (two)
+      ptr[i >> 1] = make_float4(v.re.x, v.im.x, v.re.y, v.im.y);
+    else
+      reinterpret_cast<float2*>(ptr)[i] = make_float2(v.re.x, v.im.x);
+  }
+};
+
+// rows p and p+1 of a complex array (element k of row p at p*rowstride + k)
+struct P2RowLoad {
+  const float2* ptr;
+  unsigned rowstride;
+  unsigned n;
+  int Lin;  // valid elements per row
+  int np;
+  __device__ __forceinline__ float2 one(int p, int k, unsigned& bad) const {
+    const unsigned i = (unsigned)p * rowstride + (unsigned)k;
+    const bool want = p < np && k < Lin;
+    const bool ok = want && i < n;
+    bad |= (unsigned)(want && !ok);
+    return ok ? ptr[i] : make_float2(0.f, 0.f);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Generation pass 1: counter-based (or buffered) noise x sqrt(lambda) on the R2C half
+// spectrum, backward transform along the last axis, pruned store (R2CNoise semantics,
+// r2cfieldbackend.hh:305-325 fed by matrix.hh:375-404).  Pencils are k0 (fastest) per
+// outer block k1 (3D); one Philox call per pencil serves elements j and j + L/2.
+// ---------------------------------------------------------------------------
+struct PhiloxKeys {
+  uint32_t kx[10], ky[10];
+};
+
+__device__ __forceinline__ uint4 philox_rk(uint4 c, const PhiloxKeys& k) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+    c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ k.kx[r], (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k.ky[r],
+                   (uint32_t)p0);
+  }
+  return c;
+}
+
+// Box-Muller (u1 = (a + 1/2) 2^-32 in (0, 1], u2 from the top 24 bits of b), fast
+// intrinsics; the radius uses x * rsqrt(x) with x clamped away from 0
+__device__ __forceinline__ float2 box_muller_fast(uint32_t a, uint32_t b) {
+  const float u1 = fmaf(__uint2float_rn(a), 2.3283064365386963e-10f, 1.1641532182693481e-10f);
+  const float x = fmaxf(-1.3862943611198906f * __log2f(u1), 1e-30f);  // -2 ln u1
+  const float rad = x * rsqrtf(x);
+  const float u2 = __uint_as_float(0x3f800000u | (b >> 9)) - 1.0f;  // [0, 1)
+  float s, c;
+  __sincosf(fmaf(6.283185307179586f, u2, -3.141592653589793f), &s, &c);
+  return make_float2(rad * c, rad * s);
+}
+
+template <int DIM, int LAYOUT, bool TRANSP>
+struct P2Noise {
+  // LAYOUT: 1 = DCT prod(T/2+1) eigenvalues (mirrored lookup), 0 = R2C half spectrum,
+  // 2 = full DFT spectrum (dftmatrixbackend.hh:303-307)
+  int ext0, ext1, ext2;
+  int T0c, D0, D1;
+  const float* sq;
+  const double* noise;
+  unsigned nsq, nnoise;
+  int np;
+  PhiloxKeys keys;
+  __device__ __forceinline__ unsigned stored(int k0, int k1, int kl) const {
+    if (DIM == 2) return (unsigned)k0 + (unsigned)T0c * (unsigned)kl;
+    if (TRANSP) return (unsigned)k0 + (unsigned)T0c * ((unsigned)kl + (unsigned)ext2 * (unsigned)k1);
+    return (unsigned)k0 + (unsigned)T0c * ((unsigned)k1 + (unsigned)ext1 * (unsigned)kl);
+  }
+  __device__ __forceinline__ unsigned lam_index(int k0, int k1, int kl) const {
+    const int a1 = DIM == 3 ? k1 : kl, a2 = DIM == 3 ? kl : 0;
+    if (LAYOUT == 1) {
+      const int m1 = a1 <= ext1 / 2 ? a1 : ext1 - a1;
+      const int m2 = DIM == 3 ? (a2 <= ext2 / 2 ? a2 : ext2 - a2) : 0;
+      return (unsigned)k0 + (unsigned)D0 * ((unsigned)m1 + (unsigned)D1 * (unsigned)m2);
+    }
+    if (LAYOUT == 2) return (unsigned)k0 + (unsigned)ext0 * ((unsigned)a1 + (unsigned)ext1 * (unsigned)a2);
+    return (unsigned)k0 + (unsigned)T0c * ((unsigned)a1 + (unsigned)ext1 * (unsigned)a2);
+  }
+  // (lambda A, lambda B) and the self-conjugate rule for both pencils at last-axis kl
+  __device__ __forceinline__ P2 scale(int k0, int k1, int kl, float2 rA, float2 rB, unsigned& bad) const {
+    const unsigned li = lam_index(k0, k1, kl);
+    const bool vb = k0 + 1 < np;
+    const bool okA = li < nsq, okB = !vb || li + 1 < nsq;
+    bad |= (unsigned)(!okA || !okB);
+    const float lA = okA ? sq[li] : 0.f;
+    const float lB = (vb && okB) ? sq[li + 1] : 0.f;
+    const int a1 = DIM == 3 ? k1 : kl, a2 = DIM == 3 ? kl : 0;
+    const bool sc12 = (a1 == 0 || 2 * a1 == ext1) && (DIM < 3 || a2 == 0 || 2 * a2 == ext2);
+    const bool scA = sc12 && (k0 == 0 || 2 * k0 == ext0);
+    const bool scB = sc12 && (2 * (k0 + 1) == ext0);
+    const float h = 0.70710678118654752f;
+    const float sA = scA ? lA : lA * h, sB = scB ? lB : lB * h;
+    P2 o;
+    o.re = f2mul(make_float2(sA, sB), make_float2(rA.x, rB.x));
+    o.im = make_float2(scA ? 0.f : sA * rA.y, scB ? 0.f : sB * rB.y);
+    return o;
+  }
+  // elements j and j + L/2 of pencils (p, p+1); pencil = k0, outer = k1
+  template <int L>
+  __device__ __forceinline__ void load2(int p, int j, int o, P2& x0, P2& x1, unsigned& bad) const {
+    const int k0 = p, k1 = DIM == 3 ? o : 0;
+    constexpr int h = L / 2;
+    if (p >= np) {  // pair beyond the last pencil: zero input, no lookups
+      x0 = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+      x1 = x0;
+      return;
+    }
+    float2 a0, a1, b0, b1;  // normals: pencil A at j, j+h; pencil B at j, j+h
+    if (noise) {
+      const unsigned s0 = stored(k0, k1, j), s1 = stored(k0, k1, j + h);
+      const bool vb = k0 + 1 < np;
+      const unsigned top = vb ? 2u * s0 + 3u : 2u * s0 + 1u, top1 = vb ? 2u * s1 + 3u : 2u * s1 + 1u;
+      const bool ok = top < nnoise && top1 < nnoise;
+      bad |= (unsigned)!ok;
+      double2 n00 = make_double2(0, 0), n01 = n00, n10 = n00, n11 = n00;
+      if (ok) {
+        const double2* nz2 = reinterpret_cast<const double2*>(noise);
+        n00 = nz2[s0];
+        n10 = nz2[s1];
+        if (vb) {
+          n01 = nz2[s0 + 1];
+          n11 = nz2[s1 + 1];
+        }
+      }
+      a0 = make_float2((float)n00.x, (float)n00.y);
+      a1 = make_float2((float)n10.x, (float)n10.y);
+      b0 = make_float2((float)n01.x, (float)n01.y);
+      b1 = make_float2((float)n11.x, (float)n11.y);
+    } else {
+      const unsigned si = stored(k0, k1, j);
+      const uint4 cA = philox_rk(make_uint4(si, 0u, 0x70616972u, 0u), keys);
+      const uint4 cB = philox_rk(make_uint4(si + 1u, 0u, 0x70616972u, 0u), keys);
+      a0 = box_muller_fast(cA.x, cA.y);
+      a1 = box_muller_fast(cA.z, cA.w);
+      b0 = box_muller_fast(cB.x, cB.y);
+      b1 = box_muller_fast(cB.z, cB.w);
+    }
+    x0 = scale(k0, k1, j, a0, b0, bad);
+    x1 = scale(k0, k1, j + h, a1, b1, bad);
+  }
+};
+
+template <int L, class Ld>
+__global__ void __launch_bounds__(kP2Threads, 2)
+    kp2_noise(const float4* __restrict__ twg, long long ntiles, int tpo, int Lout, Ld ld, P2ArrStore st) {
+  using G = P2Geom<L>;
+  extern __shared__ __align__(16) float4 p2_smem[];
+  float4* buf = p2_smem;
+  float4* tw = p2_smem + G::Q * G::PLQ;
+  p2_copy_table(tw, twg, G::NTW);
+  __syncthreads();
+  const int q = threadIdx.x % G::Q, u = threadIdx.x / G::Q;
+  unsigned bad = 0;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int o = (int)(tile / tpo);
+    const int p = (int)(tile - (long long)o * tpo) * G::NP + 2 * q;
+    P2 v[8];
+#pragma unroll
+    for (int r = 0; r < 4; r++) ld.template load2<L>(p, u + r * G::TP, o, v[r], v[r + 4], bad);
+    p2_transform<L, +1>(v, buf, tw, u, q, [&](int j, const P2& x) {
+      if (j < Lout) st.store(p, j, o, x, bad);
+    });
+  }
+  p2_report(bad);
+}
+
+// ---------------------------------------------------------------------------
+// Strided complex pass (pencils p, p+1 adjacent), e.g. the middle generation pass.
+// ---------------------------------------------------------------------------
+template <int L, int S>
+__global__ void __launch_bounds__(kP2Threads, 2)
+    kp2_c2c(const float4* __restrict__ twg, long long ntiles, int tpo, int Lout, P2ArrLoad ld, P2ArrStore st) {
+  using G = P2Geom<L>;
+  extern __shared__ __align__(16) float4 p2_smem[];
+  float4* buf = p2_smem;
+  float4* tw = p2_smem + G::Q * G::PLQ;
+  p2_copy_table(tw, twg, G::NTW);
+  __syncthreads();
+  const int q = threadIdx.x % G::Q, u = threadIdx.x / G::Q;
+  unsigned bad = 0;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int o = (int)(tile / tpo);
+    const int p = (int)(tile - (long long)o * tpo) * G::NP + 2 * q;
+    P2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) v[r] = ld.load(p, u + r * G::TP, o, bad);
+    p2_transform<L, S>(v, buf, tw, u, q, [&](int j, const P2& x) {
+      if (j < Lout) st.store(p, j, o, x, bad);
+    });
+  }
+  p2_report(bad);
+}
+
+// ---------------------------------------------------------------------------
+// Complex-to-real rows (2L reals from L+1 complex, FFTW c2r semantics: Im of the DC
+// and Nyquist inputs ignored), rows p and p+1 per pair, threads along the row.
+// Store(p, m, x0, x1) receives reals 2m and 2m+1 of row p.
+// ---------------------------------------------------------------------------
+template <int L, class St>
+__global__ void __launch_bounds__(kP2Threads, 2)
+    kp2_c2r(const float4* __restrict__ twg, long long ntiles, int Lout, P2RowLoad ld, St st) {
+  using G = P2Geom<L>;
+  extern __shared__ __align__(16) float4 p2_smem[];
+  float4* buf = p2_smem;
+  float4* tw = p2_smem + G::Q * G::PLQ;
+  const float4* twT = tw + G::NTW;  // exp(+2 pi i m / 2L), m < L
+  p2_copy_table(tw, twg, G::NTW + L);
+  __syncthreads();
+  const int u = threadIdx.x % G::TP, q = threadIdx.x / G::TP;
+  unsigned bad = 0;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int p = (int)tile * G::NP + 2 * q;
+    P2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const int m = u + r * G::TP;
+      float2 xa = ld.one(p, m, bad), xb = ld.one(p + 1, m, bad);
+      float2 ya = ld.one(p, L - m, bad), yb = ld.one(p + 1, L - m, bad);
+      if (m == 0) {
+        xa.y = 0.f;
+        xb.y = 0.f;
+        ya.y = 0.f;
+        yb.y = 0.f;
+      }
+      const P2 X = p2_ab(xa, xb), Y = p2_ab(ya, yb);
+      // s = X + conj(Y), d = X - conj(Y), t = d w, Z = s + i t
+      const P2 s = {f2add(X.re, Y.re), f2sub(X.im, Y.im)};
+      const P2 d = {f2sub(X.re, Y.re), f2add(X.im, Y.im)};
+      const P2 t = ptw(d, twT[m]);
+      v[r] = {f2sub(s.re, t.im), f2add(s.im, t.re)};
+    }
+    p2_transform<L, +1>(v, buf, tw, u, q, [&](int m, const P2& z) {
+      if (2 * m < Lout) st.store(p, m, z, bad);
+    });
+  }
+  p2_report(bad);
+}
+
+// field rows of n0 reals (row p at p * n0), value transform applied
+struct P2FieldStore {
+  float* out;
+  int n0;
+  int transform;
+  float boxcox;
+  unsigned n;
+  int np;
+  int Lout;
+  int vec;  // out is 8-byte aligned and n0 is even: pairs are stored as float2
+  __device__ __forceinline__ void row(int p, int m, float a, float b, unsigned& bad) const {
+    if (p >= np) return;
+    if (transform) {
+      a = apply_mutator<float>(transform, boxcox, a);
+      b = apply_mutator<float>(transform, boxcox, b);
+    }
+    const unsigned i = (unsigned)p * (unsigned)n0 + 2u * (unsigned)m;
+    const bool two = 2 * m + 1 < Lout;
+    const bool ok = i + (two ? 1u : 0u) < n;
+    bad |= (unsigned)!ok;
+    if (!ok) return;
+    if (two && vec)
+      *reinterpret_cast<float2*>(out + i) = make_float2(a, b);
+    else {
+      out[i] = a;
+      if (two) out[i + 1] = b;
+    }
+  }
+  __device__ __forceinline__ void store(int p, int m, const P2& z, unsigned& bad) const {
+    row(p, m, z.re.x, z.im.x, bad);
+    row(p + 1, m, z.re.y, z.im.y, bad);
+  }
+};
+
+}  // namespace pf
