@@ -673,28 +673,58 @@ static pf_status build_spectrum(pf_plan* P) {
   const uint64_t full = g.mb == PF_MATRIX_DFT ? g.N : g.Nc;
   TRY(workspace(P, 0, full * sizeof(double2), &A));
   TRY(workspace(P, 1, full * sizeof(double2), &Bw));
-  if (g.mb == PF_MATRIX_DCT || g.mb == PF_MATRIX_R2C) {
-    const bool dct = g.mb == PF_MATRIX_DCT;
+  cl.rowmod = g.T[1];
+  if (g.mb == PF_MATRIX_DCT) {
+    // Even torus in every dimension (DCT-I, dctmatrixbackend.hh:240-272): the covariance is
+    // evaluated only on the prod(T_i/2+1) non-mirrored cells; each later pass reads its
+    // axis through the mirror j -> T - j and keeps the T/2+1 outputs the DCT-I needs.
+    const int T0c = g.T0c;
+    const int D1 = dim >= 2 ? g.T[1] / 2 + 1 : 1, D2 = dim >= 3 ? g.T[2] / 2 + 1 : 1;
+    const long long rows = (long long)D1 * D2;
+    cl.rowmod = D1;
+    TRY((run_freal<double, true>(P, "spec_r2c_cov", g.T[0], T0c, rows, cl, arr_store<double2>(P, A, 1, 0, T0c),
+                                 rows * T0c * 16.0)));
+    spec = (double2*)A;
+    if (dim >= 2) {
+      MirrorLoad<double2> ml{(const double2*)A, (unsigned)T0c, (unsigned)((long long)T0c * D1), 1u,
+                             (unsigned)std::min<size_t>(cap_of(P, A) / sizeof(double2), 0xffffffffu), g.T[1]};
+      TRY((run_fpass<double, -1, -1, false, false>(P, "spec_c2c_d1", g.T[1], D1, T0c, D2, ml, NoMid(),
+                                                   arr_store<double2>(P, Bw, T0c, (long long)T0c * D1, 1),
+                                                   (double)T0c * D2 * (D1 + D1) * 16.0)));
+      spec = (double2*)Bw;
+      if (dim == 3) {
+        const long long inner = (long long)T0c * D1;
+        MirrorLoad<double2> m2{(const double2*)Bw, (unsigned)inner, 0u, 1u,
+                               (unsigned)std::min<size_t>(cap_of(P, Bw) / sizeof(double2), 0xffffffffu), g.T[2]};
+        TRY((run_fpass<double, -1, -1, false, false>(P, "spec_c2c_d2", g.T[2], D2, inner, 1, m2, NoMid(),
+                                                     arr_store<double2>(P, A, inner, 0, 1),
+                                                     (double)inner * (D2 + D2) * 16.0)));
+        spec = (double2*)A;
+      }
+    }
+  } else if (g.mb == PF_MATRIX_R2C) {
+    const bool dct = false;
     const int T0c = g.T0c;
     const long long rows = (long long)(g.N / (uint64_t)g.T[0]);
     // dimension 0: covariance evaluation fused into the R2C load
-    TRY((run_real_pass<double, true>(P, "spec_r2c_cov", g.T[0], T0c, rows, cl,
-                                     arr_store<double2>(P, A, 1, 0, T0c), rows * T0c * 16.0)));
+    TRY((run_freal<double, true>(P, "spec_r2c_cov", g.T[0], T0c, rows, cl, arr_store<double2>(P, A, 1, 0, T0c),
+                                 rows * T0c * 16.0)));
     spec = (double2*)A;
     if (dim >= 2) {
       const int L1 = g.T[1], L1o = dct ? g.T[1] / 2 + 1 : g.T[1];
       const long long outer = dim == 3 ? g.T[2] : 1;
-      TRY((run_pass<double, false>(P, "spec_c2c_d1", L1, L1o, T0c, outer, -1, -1,
-                                   arr_load<double2>(P, A, T0c, (long long)T0c * L1, 1, L1), NoMid(),
-                                   arr_store<double2>(P, Bw, T0c, (long long)T0c * L1o, 1),
-                                   (double)T0c * outer * (L1 + L1o) * 16.0)));
+      TRY((run_fpass<double, -1, -1, false, false>(P, "spec_c2c_d1", L1, L1o, T0c, outer,
+                                                   arr_load<double2>(P, A, T0c, (long long)T0c * L1, 1, L1), NoMid(),
+                                                   arr_store<double2>(P, Bw, T0c, (long long)T0c * L1o, 1),
+                                                   (double)T0c * outer * (L1 + L1o) * 16.0)));
       spec = (double2*)Bw;
       if (dim == 3) {
         const int L2 = g.T[2], L2o = dct ? g.T[2] / 2 + 1 : g.T[2];
         const long long inner = (long long)T0c * L1o;
-        TRY((run_pass<double, false>(P, "spec_c2c_d2", L2, L2o, inner, 1, -1, -1,
-                                     arr_load<double2>(P, Bw, inner, 0, 1, L2), NoMid(),
-                                     arr_store<double2>(P, A, inner, 0, 1), (double)inner * (L2 + L2o) * 16.0)));
+        TRY((run_fpass<double, -1, -1, false, false>(P, "spec_c2c_d2", L2, L2o, inner, 1,
+                                                     arr_load<double2>(P, Bw, inner, 0, 1, L2), NoMid(),
+                                                     arr_store<double2>(P, A, inner, 0, 1),
+                                                     (double)inner * (L2 + L2o) * 16.0)));
         spec = (double2*)A;
       }
     }

@@ -230,6 +230,24 @@ struct ArrLoad {
   }
 };
 
+// ArrLoad over an array that holds only the indices j <= T/2 of an even sequence of
+// period T along the pencil axis: element j reads index min(j, T - j)
+template <typename S>
+struct MirrorLoad {
+  const S* ptr;
+  unsigned jstride, ostride, rowstride;
+  unsigned n;
+  int T;
+  template <typename T_>
+  __device__ __forceinline__ cx<T_> load(long long p, int j, long long o) const {
+    const int m = j <= T - j ? j : T - j;
+    const unsigned i = (unsigned)p * rowstride + (unsigned)m * jstride + (unsigned)o * ostride;
+    if (!in_bounds32(i, n)) return mk<T_>(0, 0);
+    const S v = ptr[i];
+    return mk<T_>((T_)v.x, (T_)v.y);
+  }
+};
+
 template <typename S>
 struct ArrStore {
   S* ptr;
@@ -528,10 +546,12 @@ __device__ __forceinline__ double cov_at(const CovParams& c, int j0, int j1, int
 // row p of the torus (dims 1..d-1 flattened), element j along dim 0
 struct CovRowLoad {
   CovParams c;
+  int rowmod;  // rows enumerate (j1, j2) with j1 = p % rowmod (T1 for the full torus,
+               // T1/2+1 when only the non-mirrored rows of an even torus are needed)
   template <typename T>
   __device__ __forceinline__ T real(long long p, int j) const {
-    const int j1 = c.dim > 1 ? (int)(p % c.T[1]) : 0;
-    const int j2 = c.dim > 2 ? (int)(p / c.T[1]) : 0;
+    const int j1 = c.dim > 1 ? (int)(p % rowmod) : 0;
+    const int j2 = c.dim > 2 ? (int)(p / rowmod) : 0;
     return (T)cov_at(c, j, j1, j2);
   }
   template <typename T>

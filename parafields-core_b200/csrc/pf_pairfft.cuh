@@ -22,6 +22,16 @@
 namespace pf {
 
 constexpr int kP2Threads = 256;
+// resident CTAs per SM the register allocation is sized for (per kernel family)
+#ifndef PF_P2_MIN_NOISE
+#define PF_P2_MIN_NOISE 4
+#endif
+#ifndef PF_P2_MIN_C2C
+#define PF_P2_MIN_C2C 3
+#endif
+#ifndef PF_P2_MIN_C2R
+#define PF_P2_MIN_C2R 3
+#endif
 
 struct P2 {
   float2 re, im;
@@ -377,7 +387,7 @@ struct P2Noise {
 };
 
 template <int L, class Ld>
-__global__ void __launch_bounds__(kP2Threads, 2)
+__global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
     kp2_noise(const float4* __restrict__ twg, long long ntiles, int tpo, int Lout, Ld ld, P2ArrStore st) {
   using G = P2Geom<L>;
   extern __shared__ __align__(16) float4 p2_smem[];
@@ -404,7 +414,7 @@ __global__ void __launch_bounds__(kP2Threads, 2)
 // Strided complex pass (pencils p, p+1 adjacent), e.g. the middle generation pass.
 // ---------------------------------------------------------------------------
 template <int L, int S>
-__global__ void __launch_bounds__(kP2Threads, 2)
+__global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
     kp2_c2c(const float4* __restrict__ twg, long long ntiles, int tpo, int Lout, P2ArrLoad ld, P2ArrStore st) {
   using G = P2Geom<L>;
   extern __shared__ __align__(16) float4 p2_smem[];
@@ -433,7 +443,7 @@ __global__ void __launch_bounds__(kP2Threads, 2)
 // Store(p, m, x0, x1) receives reals 2m and 2m+1 of row p.
 // ---------------------------------------------------------------------------
 template <int L, class St>
-__global__ void __launch_bounds__(kP2Threads, 2)
+__global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2R)
     kp2_c2r(const float4* __restrict__ twg, long long ntiles, int Lout, P2RowLoad ld, St st) {
   using G = P2Geom<L>;
   extern __shared__ __align__(16) float4 p2_smem[];
