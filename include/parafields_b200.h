@@ -241,6 +241,36 @@ pf_status pf_generate(pf_plan* plan, const double* noise, int32_t noise_mem, uin
 pf_status pf_generate_batch(pf_plan* plan, uint64_t seed, int32_t count, void* out,
                             int32_t out_mem, int32_t apply_transform);
 
+/* Ensembles: many independent fields, each with its own size and covariance, generated
+ * together.  In the reference every field is its own RandomField and generate() call
+ * (randomfield.hh:512-558, matrix.hh:330-421); here one handle plans them all, builds
+ * every FP64 spectrum once, captures the realization passes of all fields into one CUDA
+ * graph (branches on several streams) and replays that graph with one launch per call.
+ * All descriptors must share a precision and use the R2C field backend.  Field i of call
+ * c (c = 1, 2, ...) is the counter-based realization keyed by seed + i with the call
+ * number mixed into the counters, so calls draw new, reproducible realizations. */
+typedef struct pf_ensemble pf_ensemble;
+pf_status pf_ensemble_create(const pf_field_desc* descs, int32_t count, uint64_t seed,
+                             pf_ensemble** ensemble);
+void pf_ensemble_destroy(pf_ensemble* ensemble);
+/* count, total cells, and offsets[count + 1] (field i at [offsets[i], offsets[i+1])) */
+pf_status pf_ensemble_info(const pf_ensemble* ensemble, int32_t* count, uint64_t* total_cells,
+                           uint64_t* offsets);
+/* fillTransformedMatrix for every field; `stats` (count entries) and `failed` may be NULL.
+ * Returns PF_ERR_NEG_EIGEN if any field without embedding.approximate has negative
+ * eigenvalues (the other fields are still built). */
+pf_status pf_ensemble_spectra(pf_ensemble* ensemble, pf_eig_stats* stats, int32_t* failed);
+/* One realization of every field, concatenated into `out` (memory `out_mem`; NULL keeps
+ * them in the device buffer of pf_ensemble_device_output).  The first call captures the
+ * graph; every call is one graph launch.  Synchronous. */
+pf_status pf_ensemble_generate(pf_ensemble* ensemble, void* out, int32_t out_mem);
+/* Replays the captured graph on `stream` (a cudaStream_t used as given; 0 is the legacy
+ * default stream) without waiting. */
+pf_status pf_ensemble_launch(pf_ensemble* ensemble, void* stream);
+const void* pf_ensemble_device_output(const pf_ensemble* ensemble);
+/* kernel launches inside one replay of the graph */
+uint64_t pf_ensemble_launches_per_replay(const pf_ensemble* ensemble);
+
 /* Matrix::operator* / multiplyRoot (matrix.hh:142-176, 1443-1573) and the torus
  * inverse multiplyInverseExtended (matrix.hh:1587-1646).  `in` and `out` hold
  * prod(cells) values of type `precision` (PF_PREC_F64: double, PF_PREC_F32: float);

@@ -6,11 +6,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <complex>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <type_traits>
 #include <string>
@@ -194,8 +196,6 @@ struct pf_plan {
   bool spare_valid = false;
   void* spare = nullptr;
   size_t spare_cap = 0;
-  // twiddles per (length, element size)
-  std::map<std::pair<int, int>, void*> tw;
   // CG scratch
   CgScratch cg;
   // profiling
@@ -204,6 +204,10 @@ struct pf_plan {
   std::vector<cudaEvent_t> evpool;
   uint64_t launches = 0;
   uint64_t bytes_held = 0;
+  // device word mixed into the noise counters (ensembles replaying a captured graph)
+  const unsigned* epoch = nullptr;
+  // ws[0..1] are lent by an ensemble for one spectrum build (not freed by the plan)
+  bool borrowed_ws = false;
 };
 
 static pf_status dalloc(pf_plan* P, void** p, size_t bytes) {
@@ -239,12 +243,42 @@ static pf_status workspace(pf_plan* P, int i, size_t bytes, void** out) {
   return PF_OK;
 }
 
+// Process-wide cache of the constant tables (twiddles, Bluestein chirps, paired-pass
+// twiddles): key (device, length, kind) -> device buffer.  Tables are immutable and shared
+// by every plan on the device; they live until the process exits.
+static std::mutex g_tab_mu;
+static std::map<std::tuple<int, int, int>, void*> g_tab;
+
+static void* tab_find(int dev, int L, int kind) {
+  std::lock_guard<std::mutex> lk(g_tab_mu);
+  auto it = g_tab.find(std::make_tuple(dev, L, kind));
+  return it == g_tab.end() ? nullptr : it->second;
+}
+
+static pf_status tab_put(int dev, int L, int kind, const void* host, size_t bytes, void** out) {
+  void* d = nullptr;
+  if (cudaMalloc(&d, bytes) != cudaSuccess) return fail(PF_ERR_OOM, "table of %zu bytes", bytes);
+  if (cudaMemcpy(d, host, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    return fail(PF_ERR_CUDA, "table upload failed");
+  }
+  std::lock_guard<std::mutex> lk(g_tab_mu);
+  auto key = std::make_tuple(dev, L, kind);
+  auto it = g_tab.find(key);
+  if (it != g_tab.end()) {  // another thread built it meanwhile
+    cudaFree(d);
+    *out = it->second;
+  } else {
+    g_tab[key] = d;
+    *out = d;
+  }
+  return PF_OK;
+}
+
 template <typename T>
 static pf_status twiddles(pf_plan* P, int L, const cx<T>** out) {
-  auto key = std::make_pair(L, (int)sizeof(T));
-  auto it = P->tw.find(key);
-  if (it != P->tw.end()) {
-    *out = (const cx<T>*)it->second;
+  if (void* c = tab_find(P->device, L, (int)sizeof(T))) {
+    *out = (const cx<T>*)c;
     return PF_OK;
   }
   std::vector<cx<T>> h(L);
@@ -254,12 +288,75 @@ static pf_status twiddles(pf_plan* P, int L, const cx<T>** out) {
     h[m].y = (T)-sinl(a);
   }
   void* d = nullptr;
-  size_t bytes = sizeof(cx<T>) * (size_t)L;
-  TRY(dalloc(P, &d, bytes));
-  CK(cudaMemcpy(d, h.data(), bytes, cudaMemcpyHostToDevice));
-  P->tw[key] = d;
+  TRY(tab_put(P->device, L, (int)sizeof(T), h.data(), sizeof(cx<T>) * (size_t)L, &d));
   *out = (const cx<T>*)d;
   return PF_OK;
+}
+
+// Bluestein tables of a length-L transform (layout and definitions in pf_fft.cuh, Blue):
+// one device buffer chirp | bhat | twM, cached in the twiddle map under key (L, 1000+size)
+template <typename T>
+static pf_status blue_tables(pf_plan* P, int L, Blue* out) {
+  int M = 1;
+  while (M < 2 * L - 1) M <<= 1;
+  out->M = M;
+  const int kind = 1000 + (int)sizeof(T);
+  void* d = tab_find(P->device, L, kind);
+  if (!d) {
+    typedef std::complex<double> C;
+    const double pi = 3.141592653589793238462643383279502884;
+    std::vector<C> chirp(L), f(M, C(0, 0)), w(M / 2);
+    for (int j = 0; j < L; j++) {
+      const long long q = ((long long)j * j) % (2LL * L);  // exact phase index
+      chirp[j] = std::polar(1.0, -pi * (double)q / (double)L);
+    }
+    for (int m = 0; m < M / 2; m++) w[m] = std::polar(1.0, -2.0 * pi * (double)m / (double)M);
+    int lg = 0;
+    while ((1 << lg) < M) lg++;
+    auto rev = [&](int i) {
+      int r = 0;
+      for (int k = 0; k < lg; k++) r |= ((i >> k) & 1) << (lg - 1 - k);
+      return r;
+    };
+    // b = conj(chirp) placed circularly, loaded in bit-reversed order for an in-place DIT
+    for (int n = 0; n < L; n++) {
+      f[rev(n)] = std::conj(chirp[n]);
+      if (n > 0) f[rev(M - n)] = std::conj(chirp[n]);
+    }
+    for (int len = 2; len <= M; len <<= 1) {
+      const int step = M / len;
+      for (int i = 0; i < M; i += len)
+        for (int k = 0; k < len / 2; k++) {
+          const C u = f[i + k], v = f[i + k + len / 2] * w[k * step];
+          f[i + k] = u + v;
+          f[i + k + len / 2] = u - v;
+        }
+    }
+    std::vector<cx<T>> h((size_t)L + M + M / 2);
+    for (int j = 0; j < L; j++) h[j] = cx<T>{(T)chirp[j].real(), (T)chirp[j].imag()};
+    for (int m = 0; m < M; m++) {
+      const C v = f[rev(m)] / (double)M;
+      h[L + m] = cx<T>{(T)v.real(), (T)v.imag()};
+    }
+    for (int m = 0; m < M / 2; m++) h[L + M + m] = cx<T>{(T)w[m].real(), (T)w[m].imag()};
+    TRY(tab_put(P->device, L, kind, h.data(), h.size() * sizeof(cx<T>), &d));
+  }
+  const cx<T>* base = (const cx<T>*)d;
+  out->chirp = base;
+  out->bhat = base + L;
+  out->twM = base + L + M;
+  return PF_OK;
+}
+
+// Stockham radices of L, or Bluestein tables (one pencil per tile) when L has a prime
+// factor above 13
+template <typename T>
+static pf_status schedule(pf_plan* P, int L, PassArgs* a) {
+  a->blue = Blue{0, nullptr, nullptr, nullptr};
+  if (make_radices(L, &a->rad)) return PF_OK;
+  if (L > 4096) return fail(PF_ERR_CONFIG, "transform length %d above 4096 has a prime factor above 13", L);
+  a->rad.n = 0;
+  return blue_tables<T>(P, L, &a->blue);
 }
 
 // ---------------------------------------------------------------------------
@@ -333,11 +430,14 @@ static pf_status run_pass(pf_plan* P, const char* name, int L, int Lout, long lo
   a.nouter = nouter;
   a.sign = sign;
   a.sign2 = sign2;
-  if (!make_radices(L, &a.rad)) return fail(PF_ERR_CONFIG, "transform length %d has a prime factor above 13", L);
+  TRY(schedule<T>(P, L, &a));
   tile_params(L, (int)sizeof(cx<T>), CONTIG, &a);
+  if (a.blue.M) a.B = 1;
   const cx<T>* tw = nullptr;
   TRY(twiddles<T>(P, L, &tw));
-  const size_t smem = smem_of(a, CONTIG, (int)sizeof(cx<T>));
+  // Bluestein: the tile buffer plus the M-element scratch in place of the second buffer
+  const size_t smem = a.blue.M ? ((size_t)(CONTIG ? a.pitch : L) + a.blue.M) * sizeof(cx<T>)
+                               : smem_of(a, CONTIG, (int)sizeof(cx<T>));
   if (smem > 227 * 1024) return fail(PF_ERR_CONFIG, "pencil of length %d does not fit in shared memory", L);
   auto kern = k_pass<T, CONTIG, Ld, Mid, St>;
   TRY(set_smem(kern, smem));
@@ -359,13 +459,14 @@ static pf_status run_real_pass(pf_plan* P, const char* name, int T0, int Lout, l
   a.npencil = rows;
   a.nouter = 1;
   a.sign = R2C ? -1 : 1;
-  if (!make_radices(a.L, &a.rad)) return fail(PF_ERR_CONFIG, "transform length %d has a prime factor above 13", T0);
+  TRY(schedule<T>(P, a.L, &a));
   tile_params(a.L, (int)sizeof(cx<T>), true, &a);
+  if (a.blue.M) a.B = 1;
   const cx<T>* tw = nullptr;
   const cx<T>* twT = nullptr;
   TRY(twiddles<T>(P, a.L, &tw));
   TRY(twiddles<T>(P, T0, &twT));
-  const size_t smem = smem_of(a, true, (int)sizeof(cx<T>));
+  const size_t smem = smem_of(a, true, (int)sizeof(cx<T>)) + (size_t)a.blue.M * sizeof(cx<T>);
   if (smem > 227 * 1024) return fail(PF_ERR_CONFIG, "row of length %d does not fit in shared memory", T0);
   long long grid = (rows + a.B - 1) / a.B;
   if (grid <= 0) return PF_OK;
@@ -786,10 +887,17 @@ static pf_status build_spectrum(pf_plan* P) {
   memcpy(&mn, &b, 8);
   P->stats.smallest = mn;
   // release the FP64 spectrum workspaces: they are the largest buffers of the plan
-  dfree(P, &P->ws[0], P->ws_bytes[0]);
-  P->ws_bytes[0] = 0;
-  dfree(P, &P->ws[1], P->ws_bytes[1]);
-  P->ws_bytes[1] = 0;
+  // (borrowed ones belong to the caller: an ensemble lends one pair to all its fields)
+  if (P->borrowed_ws) {
+    P->ws[0] = P->ws[1] = nullptr;
+    P->ws_bytes[0] = P->ws_bytes[1] = 0;
+    P->borrowed_ws = false;
+  } else {
+    dfree(P, &P->ws[0], P->ws_bytes[0]);
+    P->ws_bytes[0] = 0;
+    dfree(P, &P->ws[1], P->ws_bytes[1]);
+    P->ws_bytes[1] = 0;
+  }
   if (P->stats.negative > 0 && !d->approximate) {
     P->have_spec = false;
     return fail(PF_ERR_NEG_EIGEN, "negative eigenvalues in covariance matrix");
@@ -852,6 +960,7 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
   nz.sq = sizeof(T) == 8 ? (const void*)P->sq64 : (const void*)P->sq32;
   nz.noise = noise_dev;
   nz.seed = seed;
+  nz.epoch = P->epoch;
   nz.nsq = (long long)g.S;
   nz.nnoise = (long long)g.noise;
   nz.Tl = g.T[g.dim - 1];
@@ -1191,7 +1300,6 @@ void pf_plan_destroy(pf_plan* P) {
   for (int a = 0; a < 2; a++)
     for (int o = 0; o < 4; o++)
       if (P->fac[a][o]) cudaFree(P->fac[a][o]);
-  for (auto& kv : P->tw) cudaFree(kv.second);
   cg_free(P);
   for (auto& r : P->recs) {
     cudaEventDestroy(r.e0);
@@ -1595,3 +1703,5 @@ extern "C" pf_status pf_matvec_static(pf_plan* P, int32_t op, const double* in, 
   CK(cudaGetLastError());
   return PF_OK;
 }
+
+#include "pf_ensemble.inc"

@@ -250,4 +250,108 @@ __device__ cx<T>* fft_tile(cx<T>* b0, cx<T>* b1, const TileShape& ts, const Radi
   return src;
 }
 
+// ---------------------------------------------------------------------------
+// Bluestein (chirp-z) transform for lengths with a prime factor above 13
+// (L. Bluestein, "A linear filtering approach to the computation of the discrete Fourier
+// transform", 1970): with w_j = exp(s pi i (j^2 mod 2L) / L),
+//   X_k = w_k sum_j (x_j w_j) conj(w_{k-j}),
+// a circular convolution of length M >= 2L-1 (power of two) done in shared memory as an
+// in-place decimation-in-frequency FFT (natural -> bit-reversed order), a pointwise
+// product with the precomputed FFT of conj(w) (bit-reversed order, 1/M folded in), and an
+// in-place decimation-in-time inverse FFT (bit-reversed -> natural order).
+// Tables (sign -1; sign +1 uses their conjugates since conj(w) is symmetric):
+//   chirp[j] = exp(-pi i (j^2 mod 2L)/L), j < L;   bhat[m] = FFT_M(conj chirp)[rev(m)] / M;
+//   twM[m] = exp(-2 pi i m / M), m < M/2.
+// ---------------------------------------------------------------------------
+struct Blue {
+  int M;              // 0: the length is 13-smooth (Stockham stages instead)
+  const void* chirp;  // cx<T>[L]
+  const void* bhat;   // cx<T>[M]
+  const void* twM;    // cx<T>[M/2]
+};
+
+template <typename T>
+__device__ __forceinline__ cx<T> cj_if(cx<T> v, bool c) {
+  if (c) v.y = -v.y;
+  return v;
+}
+
+// in place on x[0..L) (unit stride); work holds M elements of shared memory
+template <typename T>
+__device__ void bluestein(cx<T>* x, cx<T>* work, int L, const Blue& bl, int sign) {
+  const int M = bl.M;
+  const cx<T>* chirp = (const cx<T>*)bl.chirp;
+  const cx<T>* bhat = (const cx<T>*)bl.bhat;
+  const cx<T>* twM = (const cx<T>*)bl.twM;
+  const bool c = sign > 0;
+  for (int u = threadIdx.x; u < M; u += blockDim.x)
+    work[u] = u < L ? cmul<T>(x[u], cj_if<T>(__ldg(chirp + u), c)) : mk<T>(0, 0);
+  __syncthreads();
+  // forward DIF, natural -> bit-reversed; two radix-2 stages (half H, H/2) per pass over
+  // shared memory, a last single stage when log2 M is odd
+  int half = M >> 1;
+  for (; half >= 2; half >>= 2) {
+    const int q = half >> 1;
+    for (int u = threadIdx.x; u < (M >> 2); u += blockDim.x) {
+      const int g = u / q, pos = u - g * q;
+      const int i0 = g * 2 * half + pos;
+      cx<T> a0 = work[i0], a1 = work[i0 + q], a2 = work[i0 + half], a3 = work[i0 + half + q];
+      const int ts = M / (2 * half);
+      const cx<T> wA0 = __ldg(twM + pos * ts), wA1 = __ldg(twM + (pos + q) * ts), wB = __ldg(twM + pos * 2 * ts);
+      cx<T> s0 = cadd<T>(a0, a2), d0 = cmul<T>(csub<T>(a0, a2), wA0);
+      cx<T> s1 = cadd<T>(a1, a3), d1 = cmul<T>(csub<T>(a1, a3), wA1);
+      work[i0] = cadd<T>(s0, s1);
+      work[i0 + q] = cmul<T>(csub<T>(s0, s1), wB);
+      work[i0 + half] = cadd<T>(d0, d1);
+      work[i0 + half + q] = cmul<T>(csub<T>(d0, d1), wB);
+    }
+    __syncthreads();
+  }
+  if (half == 1) {
+    for (int u = threadIdx.x; u < (M >> 1); u += blockDim.x) {
+      const cx<T> a = work[2 * u], b = work[2 * u + 1];
+      work[2 * u] = cadd<T>(a, b);
+      work[2 * u + 1] = csub<T>(a, b);
+    }
+    __syncthreads();
+  }
+  for (int u = threadIdx.x; u < M; u += blockDim.x) work[u] = cmul<T>(work[u], cj_if<T>(__ldg(bhat + u), c));
+  __syncthreads();
+  // inverse DIT, bit-reversed -> natural; radix-2 stage first when log2 M is odd, then
+  // pairs of stages (half h, 2h)
+  int h = 1;
+  int lg = 0;
+  while ((1 << lg) < M) lg++;
+  if (lg & 1) {
+    for (int u = threadIdx.x; u < (M >> 1); u += blockDim.x) {
+      const cx<T> a = work[2 * u], b = work[2 * u + 1];
+      work[2 * u] = cadd<T>(a, b);
+      work[2 * u + 1] = csub<T>(a, b);
+    }
+    __syncthreads();
+    h = 2;
+  }
+  for (; h < M; h <<= 2) {
+    for (int u = threadIdx.x; u < (M >> 2); u += blockDim.x) {
+      const int g = u / h, pos = u - g * h;
+      const int i0 = g * 4 * h + pos;
+      const int tsA = M / (2 * h), tsB = M / (4 * h);
+      const cx<T> wA = conjg<T>(__ldg(twM + pos * tsA));
+      const cx<T> wB0 = conjg<T>(__ldg(twM + pos * tsB)), wB1 = conjg<T>(__ldg(twM + (pos + h) * tsB));
+      const cx<T> a0 = work[i0], a1 = cmul<T>(work[i0 + h], wA);
+      const cx<T> a2 = work[i0 + 2 * h], a3 = cmul<T>(work[i0 + 3 * h], wA);
+      const cx<T> s0 = cadd<T>(a0, a1), d0 = csub<T>(a0, a1);
+      const cx<T> s1 = cadd<T>(a2, a3), d1 = csub<T>(a2, a3);
+      const cx<T> t0 = cmul<T>(s1, wB0), t1 = cmul<T>(d1, wB1);
+      work[i0] = cadd<T>(s0, t0);
+      work[i0 + 2 * h] = csub<T>(s0, t0);
+      work[i0 + h] = cadd<T>(d0, t1);
+      work[i0 + 3 * h] = csub<T>(d0, t1);
+    }
+    __syncthreads();
+  }
+  for (int k = threadIdx.x; k < L; k += blockDim.x) x[k] = cmul<T>(work[k], cj_if<T>(__ldg(chirp + k), c));
+  __syncthreads();
+}
+
 }  // namespace pf

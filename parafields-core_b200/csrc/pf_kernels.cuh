@@ -40,7 +40,20 @@ struct PassArgs {
   long long nouter;    // strided: outer extent
   int sign, sign2;     // first / second (fused) transform direction
   Radices rad;         // radix schedule of L
+  Blue blue;           // Bluestein tables when L has a prime factor above 13 (then B = 1)
 };
+
+// the 1D transforms of a tile: Stockham stages, or Bluestein (one pencil per tile, unit
+// stride, scratch of blue.M elements after the tile buffers); returns the result buffer
+template <typename T>
+__device__ __forceinline__ cx<T>* fft_any(cx<T>* b0, cx<T>* b1, cx<T>* work, const TileShape& ts, const PassArgs& a,
+                                          const cx<T>* __restrict__ tw, int sign) {
+  if (a.blue.M) {
+    bluestein<T>(b0, work, a.L, a.blue, sign);
+    return b0;
+  }
+  return fft_tile<T>(b0, b1, ts, a.rad, tw, sign);
+}
 
 struct NoMid {
   static constexpr bool active = false;
@@ -94,7 +107,8 @@ __global__ void __launch_bounds__(kThreads) k_pass(const PassArgs a, const cx<T>
     b0[b * ts.sb + j * ts.sj] = (p < a.npencil) ? ld.template load<T>(p, j, io) : mk<T>(0, 0);
   }
   __syncthreads();
-  cx<T>* r = fft_tile<T>(b0, b1, ts, a.rad, tw, a.sign);
+  cx<T>* wk = b1;  // Bluestein scratch (b1 is not used as a Stockham buffer then)
+  cx<T>* r = fft_any<T>(b0, b1, wk, ts, a, tw, a.sign);
   if (Mid::active) {
     for (int u = threadIdx.x; u < tot; u += blockDim.x) {
       int b, j;
@@ -109,7 +123,7 @@ __global__ void __launch_bounds__(kThreads) k_pass(const PassArgs a, const cx<T>
       if (p < a.npencil) r[b * ts.sb + j * ts.sj] = mid.template operator()<T>(p, j, io, r[b * ts.sb + j * ts.sj]);
     }
     __syncthreads();
-    r = fft_tile<T>(r, r == b0 ? b1 : b0, ts, a.rad, tw, a.sign2);
+    r = fft_any<T>(r, r == b0 ? b1 : b0, wk, ts, a, tw, a.sign2);
   }
   const int tout = a.B * a.Lout;
   for (int u = threadIdx.x; u < tout; u += blockDim.x) {
@@ -147,7 +161,7 @@ __global__ void __launch_bounds__(kThreads) k_r2c(const PassArgs a, const cx<T>*
     b0[b * a.pitch + m] = z;
   }
   __syncthreads();
-  cx<T>* Z = fft_tile<T>(b0, b1, ts, a.rad, tw, -1);
+  cx<T>* Z = fft_any<T>(b0, b1, b1 + a.B * a.pitch, ts, a, tw, -1);
   cx<T>* X = (Z == b0) ? b1 : b0;
   const int L = a.L;
   for (int u = threadIdx.x; u < a.B * (L + 1); u += blockDim.x) {
@@ -200,7 +214,7 @@ __global__ void __launch_bounds__(kThreads) k_c2r(const PassArgs a, const cx<T>*
     b0[b * a.pitch + k] = mk<T>(s.x - t.y, s.y + t.x);  // s + i t
   }
   __syncthreads();
-  cx<T>* z = fft_tile<T>(b0, b1, ts, a.rad, tw, +1);
+  cx<T>* z = fft_any<T>(b0, b1, b1 + a.B * a.pitch, ts, a, tw, +1);
   for (int u = threadIdx.x; u < a.B * a.Lout; u += blockDim.x) {
     const int b = u / a.Lout, j = u - b * a.Lout;
     const long long p = p0 + b;
@@ -607,8 +621,10 @@ __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, double& r1, d
   r2 = rad * s;
 }
 
-__device__ __forceinline__ uint4 pair_counter(uint64_t si) {
-  return make_uint4((uint32_t)si, (uint32_t)(si >> 32), 0x70616972u, 0u);
+// counter of the frequency pair whose first member has stored index si; `epoch` (0 for
+// single calls) distinguishes the realizations of repeated launches of a captured graph
+__device__ __forceinline__ uint4 pair_counter(uint64_t si, uint32_t epoch) {
+  return make_uint4((uint32_t)si, (uint32_t)(si >> 32), 0x70616972u, epoch);
 }
 
 // SplitMix64 finaliser (Steele, Lea, Flood, "Fast splittable pseudorandom number
@@ -620,14 +636,14 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 }
 
 // 128 random bits for the frequency pair whose first member has stored index si
-__device__ __forceinline__ uint4 pair_bits(uint64_t seed, uint64_t si) {
+__device__ __forceinline__ uint4 pair_bits(uint64_t seed, uint64_t si, uint32_t epoch) {
 #ifdef PF_NOISE_SPLITMIX
   const uint64_t s = mix64(seed ^ 0x5851f42d4c957f2dull);
   const uint64_t a = mix64(s + (2 * si) * 0x9e3779b97f4a7c15ull);
   const uint64_t b = mix64(s + (2 * si + 1) * 0x9e3779b97f4a7c15ull);
   return make_uint4((uint32_t)a, (uint32_t)(a >> 32), (uint32_t)b, (uint32_t)(b >> 32));
 #else
-  return philox4x32_10(pair_counter(si), make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+  return philox4x32_10(pair_counter(si, epoch), make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
 #endif
 }
 
@@ -652,6 +668,7 @@ struct R2CNoise {
   const void* sq;     // sqrt(lambda), float or double per the pass precision
   const double* noise;  // reference draw order, or null for the counter-based generator
   uint64_t seed;
+  const unsigned* epoch;  // device word mixed into the counters (null: 0)
   unsigned nsq, nnoise;   // buffer sizes (eigenvalues, noise doubles)
   int Tl;                 // extended cells of the last dimension (the pass axis)
   // The pass transforms along the last axis: p enumerates the other frequencies
@@ -707,7 +724,7 @@ struct R2CNoise {
       const int h = L / 2;
       const bool second = (L % 2 == 0) && j >= h;
       const unsigned si = stored(k0, k1, second ? j - h : j);
-      const uint4 c = pair_bits(seed, si);
+      const uint4 c = pair_bits(seed, si, epoch ? __ldg(epoch) : 0u);
       if (second)
         box_muller(c.z, c.w, r1, r2);
       else
@@ -730,7 +747,7 @@ struct R2CNoise {
       r3 = (T)noise[2 * s1];
       r4 = (T)noise[2 * s1 + 1];
     } else {
-      const uint4 c = pair_bits(seed, stored(k0, k1, j));
+      const uint4 c = pair_bits(seed, stored(k0, k1, j), epoch ? __ldg(epoch) : 0u);
       box_muller(c.x, c.y, r1, r2);
       box_muller(c.z, c.w, r3, r4);
     }

@@ -306,6 +306,7 @@ struct P2Noise {
   const double* noise;
   unsigned nsq, nnoise;
   int np;
+  const unsigned* epoch;  // device word mixed into the counters (null: 0)
   PhiloxKeys keys;
   __device__ __forceinline__ unsigned stored(int k0, int k1, int kl) const {
     if (DIM == 2) return (unsigned)k0 + (unsigned)T0c * (unsigned)kl;
@@ -374,8 +375,9 @@ struct P2Noise {
       b1 = make_float2((float)n11.x, (float)n11.y);
     } else {
       const unsigned si = stored(k0, k1, j);
-      const uint4 cA = philox_rk(make_uint4(si, 0u, 0x70616972u, 0u), keys);
-      const uint4 cB = philox_rk(make_uint4(si + 1u, 0u, 0x70616972u, 0u), keys);
+      const unsigned ep = epoch ? __ldg(epoch) : 0u;
+      const uint4 cA = philox_rk(make_uint4(si, 0u, 0x70616972u, ep), keys);
+      const uint4 cB = philox_rk(make_uint4(si + 1u, 0u, 0x70616972u, ep), keys);
       a0 = box_muller_fast(cA.x, cA.y);
       a1 = box_muller_fast(cA.z, cA.w);
       b0 = box_muller_fast(cB.x, cB.y);

@@ -158,6 +158,14 @@ def lib():
         "pf_profile_enable": (i32, [vp, i32]),
         "pf_profile_read": (i32, [vp, C.POINTER(KernelTime), i32, C.POINTER(i32)]),
         "pf_launch_count": (u64, [vp]),
+        "pf_ensemble_create": (i32, [C.POINTER(FieldDesc), i32, u64, C.POINTER(vp)]),
+        "pf_ensemble_destroy": (None, [vp]),
+        "pf_ensemble_info": (i32, [vp, C.POINTER(i32), C.POINTER(u64), C.POINTER(u64)]),
+        "pf_ensemble_spectra": (i32, [vp, C.POINTER(EigStats), C.POINTER(i32)]),
+        "pf_ensemble_generate": (i32, [vp, vp, i32]),
+        "pf_ensemble_launch": (i32, [vp, vp]),
+        "pf_ensemble_device_output": (vp, [vp]),
+        "pf_ensemble_launches_per_replay": (u64, [vp]),
         "pf_last_error_string": (C.c_char_p, []),
         "pf_version": (C.c_char_p, []),
     }
@@ -297,3 +305,55 @@ class Plan:
 
     def launch_count(self):
         return int(lib().pf_launch_count(self.h))
+
+
+class Ensemble:
+    """Many independent fields (own sizes and covariances) generated together: one FP64
+    spectrum per field, all realization passes replayed from one captured CUDA graph."""
+
+    def __init__(self, descs, seed=0):
+        arr = (FieldDesc * len(descs))(*descs)
+        h = C.c_void_p()
+        _check(lib().pf_ensemble_create(arr, len(descs), seed, C.byref(h)))
+        self.h = h
+        self.count = len(descs)
+        self.precision = descs[0].precision
+        n = C.c_int32()
+        tot = C.c_uint64()
+        offs = (C.c_uint64 * (self.count + 1))()
+        _check(lib().pf_ensemble_info(self.h, C.byref(n), C.byref(tot), offs))
+        self.total = int(tot.value)
+        self.offsets = np.array(offs[:], dtype=np.int64)
+
+    def spectra(self):
+        stats = (EigStats * self.count)()
+        failed = C.c_int32()
+        _check(lib().pf_ensemble_spectra(self.h, stats, C.byref(failed)))
+        return [s.as_dict() for s in stats]
+
+    def generate(self, out=None):
+        if out is None:
+            out = np.empty(self.total, dtype=np.float64 if self.precision == PREC_F64 else np.float32)
+        ptr, mem = _ptr(out)
+        _check(lib().pf_ensemble_generate(self.h, ptr, mem))
+        return out
+
+    def launch(self, stream=None):
+        _check(lib().pf_ensemble_launch(self.h, stream))
+
+    def launches_per_replay(self):
+        return int(lib().pf_ensemble_launches_per_replay(self.h))
+
+    def field(self, flat, i):
+        return flat[self.offsets[i]:self.offsets[i + 1]]
+
+    def close(self):
+        if self.h:
+            lib().pf_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -47,6 +47,11 @@ CONFIGS = {
                             anisotropy="geometric", approximate=True),
     "3d-exp-iso-notransp-pow2": dict(dim=3, cells=(64, 64, 128), covariance="exponential", corr_length=0.05,
                                      transposed=0),
+    # tori whose lengths have prime factors above 13: Bluestein transforms
+    "2d-exp-prime": dict(dim=2, cells=(131, 97), covariance="exponential", corr_length=0.1),
+    "3d-sph-prime": dict(dim=3, cells=(17, 19, 23), covariance="spherical", corr_length=0.2),
+    "2d-exp-geo-prime-long": dict(dim=2, cells=(64, 2039), covariance="exponential",
+                                  corr_length=(0.1, 0.02, -0.02, 0.05), anisotropy="geometric", approximate=True),
 }
 
 
@@ -99,7 +104,7 @@ def test_generate_parity(oracle, name, prec):
 @pytest.mark.parametrize("prec", [pfb200.PREC_F64, pfb200.PREC_F32])
 @pytest.mark.parametrize("op", [pfb200.OP_MUL, pfb200.OP_ROOT, pfb200.OP_INVEXT])
 @pytest.mark.parametrize("name", ["2d-exp-iso", "2d-sph-geo", "3d-gexp-iso-notransp", "3d-exp-geo",
-                                  "3d-matern32-axi"])
+                                  "3d-matern32-axi", "2d-exp-prime", "3d-sph-prime"])
 def test_matvec_parity(oracle, name, op, prec):
     d, P, lam, st, _ = plan_and_oracle(oracle, CONFIGS[name])
     if op == pfb200.OP_INVEXT and (lam <= 0).any():
@@ -282,7 +287,7 @@ def _box_muller(a, b, fp64):
     return rad * np.cos(ang), rad * np.sin(ang)
 
 
-def counter_noise(g, seed, fp64):
+def counter_noise(g, seed, fp64, epoch=0):
     """The device's seeded noise in the reference draw order (R2C field backend, even last
     extent): stored frequency s with last-axis index kl < T/2 takes words (x, y) of
     Philox(s, 0, 'pair', 0); its partner kl + T/2 takes words (z, w) of the same call."""
@@ -305,7 +310,8 @@ def counter_noise(g, seed, fp64):
         return k0 + T0c * (k1 + T[1] * kk)
 
     s0, s1 = stored(kl).ravel(), stored(kl + h).ravel()
-    x, y, z, w = _philox4x32_10((s0, np.zeros_like(s0), np.full_like(s0, 0x70616972), np.zeros_like(s0)), seed)
+    x, y, z, w = _philox4x32_10((s0, np.zeros_like(s0), np.full_like(s0, 0x70616972), np.full_like(s0, epoch)),
+                                seed)
     out = np.empty(int(g.noise))
     out[2 * s0], out[2 * s0 + 1] = _box_muller(x, y, fp64)
     out[2 * s1], out[2 * s1 + 1] = _box_muller(z, w, fp64)
@@ -325,3 +331,53 @@ def test_counter_noise_matches_host_philox(oracle, name, prec):
     ref, _ = oracle.generate(d, lam, counter_noise(g, seed, prec == pfb200.PREC_F64))
     out = P.generate(seed=seed)
     assert rel(out, ref) < (1e-9 if prec == pfb200.PREC_F64 else TOL32)
+
+
+# ---------------------------------------------------------------------------
+# ensembles: fields of different sizes and covariances from one captured graph
+# ---------------------------------------------------------------------------
+ENSEMBLE = [
+    dict(dim=2, cells=(131, 97), covariance="exponential", corr_length=(0.1, 0.03, -0.02, 0.06),
+         anisotropy="geometric", approximate=True),
+    dict(dim=2, cells=(128, 256), covariance="gaussian", corr_length=(0.05, 0.0, 0.0, 0.05),
+         anisotropy="geometric", approximate=True),
+    dict(dim=2, cells=(200, 150), covariance="spherical", corr_length=(0.2, 0.1, -0.1, 0.15),
+         anisotropy="geometric", approximate=True),
+    dict(dim=2, cells=(64, 64), covariance="cubic", corr_length=(0.3, 0.0, 0.0, 0.3),
+         anisotropy="geometric", approximate=True),
+    dict(dim=3, cells=(32, 24, 20), covariance="matern32", corr_length=(0.2, 0.1, 0.05),
+         anisotropy="axiparallel", approximate=True),
+]
+
+
+def test_ensemble_matches_single_field_oracle(oracle):
+    """Every field of two successive ensemble calls equals the oracle fed the host
+    reproduction of its counter-based noise (seed + i, epoch = call number)."""
+    descs = [desc_of(c, precision=pfb200.PREC_F32) for c in ENSEMBLE]
+    E = pfb200.Ensemble(descs, seed=777)
+    stats = E.spectra()
+    for call in (1, 2):
+        out = E.generate()
+        assert E.launches_per_replay() > len(descs)
+        for i, d in enumerate(descs):
+            g = oracle.resolve(d)
+            lam, ost, _ = oracle.spectrum(d)
+            assert stats[i]["negative"] == ost["negative"]
+            ref, _ = oracle.generate(d, lam, counter_noise(g, 777 + i, False, epoch=call))
+            assert rel(E.field(out, i), ref) < TOL32, (call, i)
+    E.close()
+
+
+def test_ensemble_device_replay_is_new_noise(oracle):
+    torch = pytest.importorskip("torch")
+    descs = [desc_of(c, precision=pfb200.PREC_F32) for c in ENSEMBLE[:3]]
+    E = pfb200.Ensemble(descs, seed=5)
+    E.spectra()
+    a = torch.empty(E.total, dtype=torch.float32, device="cuda")
+    b = torch.empty_like(a)
+    E.generate(a)
+    E.generate(b)
+    torch.cuda.synchronize()
+    assert not torch.equal(a, b)
+    assert abs(float(a.std()) - float(b.std())) < 0.2 * float(a.std())
+    E.close()
