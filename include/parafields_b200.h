@@ -299,6 +299,34 @@ pf_status pf_matvec_static(pf_plan* plan, int32_t op, const double* in, double* 
 pf_status pf_multiply_inverse(pf_plan* plan, const double* b, double* x, int32_t mem,
                               const pf_cg_opts* opts, pf_cg_report* report);
 
+/* Learned boundary correction of the CG preconditioner.  No counterpart in the reference
+ * (its innerCG preconditions with the torus inverse only, matrix.hh:1315-1432).  The
+ * residual-mode CG preconditions the domain-restricted covariance with the torus inverse
+ * P0 (zero-padded FFT round trip); the learned part rescales it as M = D P0 D, D a positive
+ * diagonal d(x) = exp(sum_i psi(t_i(x))), t_i the distance of cell x to the nearer face
+ * along axis i in correlation lengths and psi a 1-H-1 tanh network.  M is symmetric
+ * positive definite for all parameters, so plain PCG stays valid and remains the judge
+ * through its FP64 true residual.  Training (Adam, on the GPU) fits M b ~ x on pairs
+ * (b, x = A^-1 b) produced by plain CG, loss (1/count) sum ||M b_i - x_i||^2 / ||x_i||^2.
+ * The object refers to its plan: destroy it before the plan. */
+typedef struct pf_learned pf_learned;
+pf_status pf_learned_create(pf_plan* plan, int32_t hidden, uint64_t seed, pf_learned** learned);
+void pf_learned_destroy(pf_learned* learned);
+int32_t pf_learned_param_count(const pf_learned* learned);           /* 3 * hidden + 1 */
+pf_status pf_learned_get_params(const pf_learned* learned, double* params);  /* host */
+pf_status pf_learned_set_params(pf_learned* learned, const double* params);  /* host */
+/* loss and gradient (host array of param_count, may be NULL) over `count` pairs stored
+ * back to back (prod(cells) doubles each) in memory `mem`; fp32 selects FP32 transforms */
+pf_status pf_learned_loss_grad(pf_learned* learned, const double* B, const double* X, int32_t count,
+                               int32_t mem, int32_t fp32, double* loss, double* grad);
+/* `epochs` full-batch Adam steps; *loss_out (may be NULL) = loss after training */
+pf_status pf_learned_train(pf_learned* learned, const double* B, const double* X, int32_t count,
+                           int32_t mem, int32_t epochs, double lr, int32_t fp32, double* loss_out);
+/* z = D P0 D r (FP64 transforms) */
+pf_status pf_learned_apply(pf_learned* learned, const double* r, double* z, int32_t mem);
+/* Attaches `learned` (NULL detaches) as the preconditioner of PF_CG_RESIDUAL solves of `plan`. */
+pf_status pf_plan_set_preconditioner(pf_plan* plan, pf_learned* learned);
+
 /* ValueTransform::apply (mutators.hh:35-163) over `count` values of `precision`. */
 pf_status pf_apply_transform(pf_plan* plan, int32_t precision, void* data, uint64_t count,
                              int32_t mem);

@@ -197,3 +197,77 @@ def noise(seed, count):
     """Seeded N(0,1) doubles (numpy PCG64 + its standard normal method); the same
     buffer is fed to the oracle and to the GPU in the reference's draw order."""
     return np.random.default_rng(seed).standard_normal(int(count))
+
+
+# ---------------------------------------------------------------------------
+# learned boundary correction of the CG preconditioner: M = D P0 D (no counterpart in
+# the reference; the library's kernels are in csrc/pf_learned.cuh).  FP64 restatement of
+# its features, scaling, loss and gradient, used to check the device gradients.
+# ---------------------------------------------------------------------------
+def learned_features(desc):
+    g = resolve(desc)
+    dim = g.dim
+    lens = []
+    cl = list(desc.corr_length)
+    for i in range(3):
+        if i >= dim:
+            lens.append(1.0)
+        elif desc.anisotropy == 0:
+            lens.append(cl[0])
+        elif desc.anisotropy == 1:
+            lens.append(cl[i])
+        else:
+            lens.append(float(np.sqrt(sum(cl[i * dim + j] ** 2 for j in range(dim)))))
+    feats = []
+    for a in range(3):
+        n = g.n[a]
+        m = np.arange(n)
+        dist = np.minimum(m + 0.5, n - m - 0.5)
+        feats.append(dist * g.h[a] / lens[a])
+    return g, feats
+
+
+def learned_psi(theta, H, t):
+    t = np.asarray(t, dtype=np.float64)
+    w1, b1, w2, b2 = theta[:H], theta[H:2 * H], theta[2 * H:3 * H], theta[3 * H]
+    return np.tanh(np.outer(t, w1) + b1) @ w2 + b2
+
+
+def learned_scale(desc, theta, H):
+    g, feats = learned_features(desc)
+    dim = g.dim
+    psi = [learned_psi(theta, H, feats[a]) if a < dim else np.zeros(g.n[a]) for a in range(3)]
+    s = psi[2][:, None, None] + psi[1][None, :, None] + psi[0][None, None, :]   # (x2, x1, x0)
+    return np.exp(s).ravel()
+
+
+def learned_loss_grad(desc, lam, theta, H, B, X):
+    """L = (1/K) sum ||D P0 D b - x||^2 / ||x||^2 and dL/dtheta (P0 = torus inverse)."""
+    g, feats = learned_features(desc)
+    dim = g.dim
+    n = [g.n[0], g.n[1], g.n[2]]
+    d = learned_scale(desc, theta, H)
+    K = len(B)
+    loss = 0.0
+    gcell = np.zeros_like(d)
+    for b, x in zip(B, X):
+        v = matvec(desc, lam, 2, d * b)
+        e = d * v - x
+        xx = float(x @ x)
+        loss += float(e @ e) / xx / K
+        w = matvec(desc, lam, 2, d * e)
+        gcell += (2.0 / (xx * K)) * (e * v + b * w) * d
+    gc = gcell.reshape(n[2], n[1], n[0])
+    gprof = [gc.sum(axis=(0, 1)), gc.sum(axis=(0, 2)), gc.sum(axis=(1, 2))]
+    w1, b1, w2 = theta[:H], theta[H:2 * H], theta[2 * H:3 * H]
+    grad = np.zeros(3 * H + 1)
+    for a in range(dim):
+        t = feats[a]
+        A = np.tanh(np.outer(t, w1) + b1)                      # (m, H)
+        gp = gprof[a]
+        grad[2 * H:3 * H] += gp @ A
+        dA = (1.0 - A ** 2) * w2
+        grad[:H] += (gp * t) @ dA
+        grad[H:2 * H] += gp @ dA
+        grad[3 * H] += gp.sum()
+    return loss, grad

@@ -23,6 +23,7 @@
 #include "pf_kernels.cuh"
 #include "pf_fastfft.cuh"
 #include "pf_pairfft.cuh"
+#include "pf_learned.cuh"
 
 using namespace pf;
 
@@ -169,6 +170,8 @@ struct ProfRec {
   double bytes;
 };
 
+struct pf_learned;
+
 struct pf_plan {
   pf_field_desc desc;
   Geom g;
@@ -208,6 +211,8 @@ struct pf_plan {
   const unsigned* epoch = nullptr;
   // ws[0..1] are lent by an ensemble for one spectrum build (not freed by the plan)
   bool borrowed_ws = false;
+  // learned preconditioner of the residual-mode CG (pf_plan_set_preconditioner), not owned
+  pf_learned* learned = nullptr;
 };
 
 static pf_status dalloc(pf_plan* P, void** p, size_t bytes) {
@@ -1206,7 +1211,10 @@ static pf_status cg_matvec(pf_plan* P, int op, bool fp32, const double* in, doub
   return matvec_dev<double, double>(P, op, in, out);
 }
 
+static pf_status learned_apply(pf_learned* Lp, bool fp32, const double* r, double* z);
+
 #include "pf_cg_host.inc"
+#include "pf_learned.inc"
 
 static pf_status stage_noise(pf_plan* P, const double* noise, int noise_mem, const double** dev) {
   *dev = nullptr;

@@ -166,6 +166,15 @@ def lib():
         "pf_ensemble_launch": (i32, [vp, vp]),
         "pf_ensemble_device_output": (vp, [vp]),
         "pf_ensemble_launches_per_replay": (u64, [vp]),
+        "pf_learned_create": (i32, [vp, i32, u64, C.POINTER(vp)]),
+        "pf_learned_destroy": (None, [vp]),
+        "pf_learned_param_count": (i32, [vp]),
+        "pf_learned_get_params": (i32, [vp, vp]),
+        "pf_learned_set_params": (i32, [vp, vp]),
+        "pf_learned_loss_grad": (i32, [vp, vp, vp, i32, i32, i32, C.POINTER(C.c_double), vp]),
+        "pf_learned_train": (i32, [vp, vp, vp, i32, i32, i32, C.c_double, i32, C.POINTER(C.c_double)]),
+        "pf_learned_apply": (i32, [vp, vp, vp, i32]),
+        "pf_plan_set_preconditioner": (i32, [vp, vp]),
         "pf_last_error_string": (C.c_char_p, []),
         "pf_version": (C.c_char_p, []),
     }
@@ -350,6 +359,68 @@ class Ensemble:
     def close(self):
         if self.h:
             lib().pf_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Learned:
+    """Learned boundary correction M = D P0 D of a plan's CG preconditioner."""
+
+    def __init__(self, plan, hidden=8, seed=0):
+        h = C.c_void_p()
+        _check(lib().pf_learned_create(plan.h, hidden, seed, C.byref(h)))
+        self.h = h
+        self.plan = plan
+        self.hidden = hidden
+        self.n = int(lib().pf_learned_param_count(self.h))
+
+    @property
+    def params(self):
+        out = np.empty(self.n)
+        _check(lib().pf_learned_get_params(self.h, out.ctypes.data))
+        return out
+
+    @params.setter
+    def params(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        _check(lib().pf_learned_set_params(self.h, v.ctypes.data))
+
+    def loss_grad(self, B, X, fp32=False):
+        bptr, mem = _ptr(B)
+        xptr, _ = _ptr(X)
+        count = B.shape[0]
+        loss = C.c_double()
+        grad = np.empty(self.n)
+        _check(lib().pf_learned_loss_grad(self.h, bptr, xptr, count, mem, int(fp32), C.byref(loss),
+                                          grad.ctypes.data))
+        return loss.value, grad
+
+    def train(self, B, X, epochs, lr=0.02, fp32=True):
+        bptr, mem = _ptr(B)
+        xptr, _ = _ptr(X)
+        loss = C.c_double()
+        _check(lib().pf_learned_train(self.h, bptr, xptr, B.shape[0], mem, epochs, lr, int(fp32), C.byref(loss)))
+        return loss.value
+
+    def apply(self, r, out=None):
+        if out is None:
+            out = np.empty_like(r)
+        rptr, mem = _ptr(r)
+        optr, _ = _ptr(out)
+        _check(lib().pf_learned_apply(self.h, rptr, optr, mem))
+        return out
+
+    def attach(self, enable=True):
+        _check(lib().pf_plan_set_preconditioner(self.plan.h, self.h if enable else None))
+
+    def close(self):
+        if self.h:
+            lib().pf_learned_destroy(self.h)
             self.h = None
 
     def __del__(self):
