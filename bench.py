@@ -253,6 +253,208 @@ def run_b200(args):
         torch.distributed.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# further workloads (one JSON line each; the default run above is the headline)
+# ---------------------------------------------------------------------------
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def run_plain2d(args):
+    """Plain method, 2D: 512^2 exponential (sigma^2=1, l=0.1, isotropic), factor 2 (1024^2
+    torus), FP64, one realization from N(0,1) noise drawn on the host from a seed and fed in
+    the reference's draw order (host buffer in, host field out)."""
+    import torch
+    import pfb200
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    d = pfb200.make_desc(dim=2, cells=(512, 512), covariance="exponential", corr_length=0.1,
+                         precision=pfb200.PREC_F64)
+    P = pfb200.Plan(d)
+    P.spectrum_build()
+    g = O.resolve(d)
+    noise = torch.tensor(O.noise(20261203, g.noise)).pin_memory().numpy()
+    out = torch.empty(g.domain, dtype=torch.float64).pin_memory().numpy()
+    for _ in range(args.warmup):
+        P.generate(noise=noise, out=out)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        P.generate(noise=noise, out=out)
+    dt = (time.perf_counter() - t0) / args.steps
+    lam, _, _ = O.spectrum(d)
+    ref, _ = O.generate(d, lam, O.noise(20261203, g.noise))
+    err = float(np.linalg.norm(out - ref) / np.linalg.norm(ref))
+    O.set_threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    O.generate(d, lam, O.noise(20261203, g.noise))
+    cpu = time.perf_counter() - t0
+    print(json.dumps({"metric": "field cells/s (2D exponential 512^2, 1024^2 torus, FP64, host noise in, host field out)",
+                      "value": g.domain / dt, "unit": "cells/s", "ms_per_step": dt * 1e3, "dtype": "f64",
+                      "rel_l2_error_vs_oracle": err, "h2d_bytes_per_step": g.noise * 8,
+                      "d2h_bytes_per_step": g.domain * 8,
+                      "cpu_baseline": {"value": g.domain / cpu, "unit": "cells/s", "cores": os.cpu_count(),
+                                       "kind": "port"}}), flush=True)
+
+
+def c3_descs(count, precision, seed=20261203):
+    """Batched uneven ensemble: sides log-uniform on [128, 2048] per axis, covariance uniform over
+    {exponential, gaussian, spherical, cubic}, l ~ U[0.02, 0.3], sigma^2 ~ U[0.5, 2], geometric
+    anisotropy l * R(theta) with theta ~ U[0, pi), embedding.approximate = true."""
+    import math
+    import pfb200
+    rng = np.random.default_rng(seed)
+    covs = ["exponential", "gaussian", "spherical", "cubic"]
+    out = []
+    for _ in range(count):
+        nx, ny = (int(round(math.exp(rng.uniform(math.log(128), math.log(2048))))) for _ in range(2))
+        cov = covs[int(rng.integers(4))]
+        ell, var, th = rng.uniform(0.02, 0.3), rng.uniform(0.5, 2.0), rng.uniform(0, math.pi)
+        c, s = math.cos(th), math.sin(th)
+        out.append(pfb200.make_desc(dim=2, cells=(nx, ny), covariance=cov, variance=var,
+                                    corr_length=(ell * c, -ell * s, ell * s, ell * c), anisotropy="geometric",
+                                    approximate=True, precision=precision))
+    return out
+
+
+def run_ensemble(args):
+    """Uneven 2D fields: mixed (FP32 realizations, FP64 spectra) graph replay vs FP64 replay
+    vs the plain FP64 path (one plan and one pf_generate per field)."""
+    import torch
+    import pfb200
+    count = args.fields
+    res = {}
+    for name, prec in (("fp32", pfb200.PREC_F32), ("fp64", pfb200.PREC_F64)):
+        descs = c3_descs(count, prec)
+        E = pfb200.Ensemble(descs, seed=1)
+        t0 = time.perf_counter()
+        st = E.spectra()
+        torch.cuda.synchronize()
+        tspec = time.perf_counter() - t0
+        out = torch.empty(E.total, dtype=torch.float32 if prec else torch.float64, device="cuda")
+        E.generate(out)
+        s = torch.cuda.current_stream()
+        for _ in range(max(1, args.warmup)):
+            E.launch(s.cuda_stream)
+        e0, e1 = _events()
+        e0.record(s)
+        for _ in range(args.steps):
+            E.launch(s.cuda_stream)
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        res[name] = {"cells": E.total, "ms_per_ensemble": ms, "cells_per_s": E.total / (ms / 1e3),
+                     "spectra_s": tspec, "fields_with_negative_eigenvalues": sum(1 for x in st if x["negative"]),
+                     "launches_per_replay": E.launches_per_replay()}
+        E.close()
+        del out
+        torch.cuda.empty_cache()
+    sub = c3_descs(count, pfb200.PREC_F64)[: min(count, 256)]
+    cells, ms_tot = 0, 0.0
+    s = torch.cuda.current_stream()
+    for dsc in sub:
+        P = pfb200.Plan(dsc)
+        P.set_stream(s.cuda_stream)
+        P.spectrum_build()
+        o = torch.empty(P.info.domain_size, dtype=torch.float64, device="cuda")
+        P.generate(seed=3, out=o)
+        e0, e1 = _events()
+        e0.record(s)
+        P.generate(seed=4, out=o)
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms_tot += e0.elapsed_time(e1)
+        cells += P.info.domain_size
+        P.close()
+    res["fp64_plain_per_field"] = {"fields": len(sub), "cells": cells, "cells_per_s": cells / (ms_tot / 1e3)}
+    res["mixed_batched_vs_plain_fp64"] = res["fp32"]["cells_per_s"] / res["fp64_plain_per_field"]["cells_per_s"]
+    print(json.dumps({"metric": f"ensemble field cells/s ({count} uneven 2D fields)", "unit": "cells/s",
+                      "value": res["fp32"]["cells_per_s"], "dtype": "f32", "detail": res}), flush=True)
+
+
+def run_cinv(args):
+    """C^-1 on n^3 exponential with a seeded random rotation diag(0.15, 0.08, 0.04): plain
+    PCG vs learned-corrected PCG to the 1e-8 FP64 true residual (FP32 inner matvecs)."""
+    import torch
+    import pfb200
+    n = args.cells
+    rng = np.random.default_rng(20261203)
+    Q, R = np.linalg.qr(rng.standard_normal((3, 3)))
+    Q = Q * np.sign(np.diag(R))
+    A = Q @ np.diag([0.15, 0.08, 0.04])
+    d = pfb200.make_desc(dim=3, cells=(n, n, n), covariance="exponential", corr_length=tuple(A.ravel()),
+                         anisotropy="geometric", approximate=True)
+    P = pfb200.Plan(d)
+    st = P.spectrum_build()
+    N = P.info.domain_size
+    K_train, K_test = args.train_pairs, args.rhs
+    Bt = torch.tensor(rng.standard_normal((K_train, N)), device="cuda")
+    Xt = torch.empty_like(Bt)
+    t0 = time.perf_counter()
+    for i in range(K_train):
+        P.multiply_inverse(Bt[i], x=Xt[i], mode=pfb200.CG_RESIDUAL, tolerance=1e-8, inner_fp32=True,
+                           max_iterations=20000)
+    torch.cuda.synchronize()
+    tpairs = time.perf_counter() - t0
+    Lp = pfb200.Learned(P, hidden=8, seed=11, residual_loss=args.residual_loss)
+    loss0, _ = Lp.loss_grad(Bt, Xt, fp32=True)
+    t0 = time.perf_counter()
+    loss1 = Lp.train(Bt, Xt, epochs=args.epochs, lr=0.05, fp32=True)
+    ttrain = time.perf_counter() - t0
+    Bs = torch.tensor(rng.standard_normal((K_test, N)), device="cuda")
+    x = torch.empty(N, dtype=torch.float64, device="cuda")
+    out = {}
+    for name, attach in (("plain", False), ("learned", True)):
+        Lp.attach(attach)
+        it, res = 0, []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(K_test):
+            _, rep = P.multiply_inverse(Bs[i], x=x, mode=pfb200.CG_RESIDUAL, tolerance=1e-8, inner_fp32=True,
+                                        max_iterations=20000)
+            it += rep["iterations"]
+            res.append(rep["relative_residual"])
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[name] = {"solves_per_s": K_test / dt, "s_per_solve": dt / K_test, "iterations_per_solve": it / K_test,
+                     "max_relative_residual": max(res)}
+    Lp.attach(False)
+    print(json.dumps({"metric": f"C^-1 solves/s ({n}^3 exponential, geometric anisotropy, 1e-8 FP64 residual)",
+                      "unit": "solves/s", "value": out["plain"]["solves_per_s"], "dtype": "f32 inner / f64 residual",
+                      "eigen": st, "plain": out["plain"], "learned": out["learned"],
+                      "training": {"pairs": K_train, "pair_generation_s": tpairs, "epochs": args.epochs,
+                                   "loss": "residual norm" if args.residual_loss else "solution norm",
+                                   "train_s": ttrain, "loss_before": loss0, "loss_after": loss1}}), flush=True)
+    Lp.close()
+
+
+def run_lognormal(args):
+    """Log-normal exp(Z) realizations, 192^3 Matern nu=1.5 (l=0.1), FP32, transform applied in
+    the last pass."""
+    import torch
+    import pfb200
+    d = pfb200.make_desc(dim=3, cells=(192, 192, 192), covariance="matern32", corr_length=0.1,
+                         approximate=True, precision=pfb200.PREC_F32, transform="logNormal")
+    P = pfb200.Plan(d)
+    s = torch.cuda.current_stream()
+    P.set_stream(s.cuda_stream)
+    P.spectrum_build()
+    n = P.info.domain_size
+    out = torch.empty(n, dtype=torch.float32, device="cuda")
+    for i in range(args.warmup):
+        P.generate(seed=i, out=out, apply_transform=True)
+    e0, e1 = _events()
+    e0.record(s)
+    for i in range(args.steps):
+        P.generate(seed=100 + i, out=out, apply_transform=True)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"metric": "log-normal field cells/s (192^3, 384^3 torus, FP32)", "unit": "cells/s",
+                      "value": n / (ms / 1e3), "ms_per_step": ms, "dtype": "f32",
+                      "min": float(out.min()), "mean": float(out.mean())}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -260,11 +462,22 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="matern3d",
+                    choices=["matern3d", "plain2d", "ensemble", "cinv", "lognormal"])
+    ap.add_argument("--fields", type=int, default=2048)
+    ap.add_argument("--cells", type=int, default=128)
+    ap.add_argument("--rhs", type=int, default=4)
+    ap.add_argument("--train-pairs", type=int, default=16)
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--residual-loss", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
-    else:
+    elif args.workload == "matern3d":
         run_b200(args)
+    else:
+        {"plain2d": run_plain2d, "ensemble": run_ensemble, "cinv": run_cinv, "lognormal": run_lognormal}[
+            args.workload](args)
 
 
 if __name__ == "__main__":

@@ -307,7 +307,8 @@ pf_status pf_multiply_inverse(pf_plan* plan, const double* b, double* x, int32_t
  * along axis i in correlation lengths and psi a 1-H-1 tanh network.  M is symmetric
  * positive definite for all parameters, so plain PCG stays valid and remains the judge
  * through its FP64 true residual.  Training (Adam, on the GPU) fits M b ~ x on pairs
- * (b, x = A^-1 b) produced by plain CG, loss (1/count) sum ||M b_i - x_i||^2 / ||x_i||^2.
+ * (b, x = A^-1 b) produced by plain CG (loss: pf_learned_set_loss).  A residual-mode solve
+ * that does not converge with the learned preconditioner is repeated with P0 alone.
  * The object refers to its plan: destroy it before the plan. */
 typedef struct pf_learned pf_learned;
 pf_status pf_learned_create(pf_plan* plan, int32_t hidden, uint64_t seed, pf_learned** learned);
@@ -322,6 +323,11 @@ pf_status pf_learned_loss_grad(pf_learned* learned, const double* B, const doubl
 /* `epochs` full-batch Adam steps; *loss_out (may be NULL) = loss after training */
 pf_status pf_learned_train(pf_learned* learned, const double* B, const double* X, int32_t count,
                            int32_t mem, int32_t epochs, double lr, int32_t fp32, double* loss_out);
+/* Training loss: residual_norm = 0 (default) uses ||M b - x||^2 / ||x||^2; 1 uses
+ * ||A (M b - x)||^2 / ||b||^2.  The residual norm is not invariant to a scalar factor of M
+ * (PCG is): where ||A P0 b - b|| > ||b||, as on the 48^3 and 128^3 exponential test cases,
+ * it drives D toward 0 (loss -> 1) and the trained M is useless for CG. */
+pf_status pf_learned_set_loss(pf_learned* learned, int32_t residual_norm);
 /* z = D P0 D r (FP64 transforms) */
 pf_status pf_learned_apply(pf_learned* learned, const double* r, double* z, int32_t mem);
 /* Attaches `learned` (NULL detaches) as the preconditioner of PF_CG_RESIDUAL solves of `plan`. */

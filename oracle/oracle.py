@@ -241,8 +241,9 @@ def learned_scale(desc, theta, H):
     return np.exp(s).ravel()
 
 
-def learned_loss_grad(desc, lam, theta, H, B, X):
-    """L = (1/K) sum ||D P0 D b - x||^2 / ||x||^2 and dL/dtheta (P0 = torus inverse)."""
+def learned_loss_grad(desc, lam, theta, H, B, X, residual=False):
+    """L = (1/K) sum ||D P0 D b - x||^2 / ||x||^2 (or ||A(D P0 D b - x)||^2 / ||b||^2 with
+    residual=True) and dL/dtheta (P0 = torus inverse, A the restricted covariance)."""
     g, feats = learned_features(desc)
     dim = g.dim
     n = [g.n[0], g.n[1], g.n[2]]
@@ -253,10 +254,16 @@ def learned_loss_grad(desc, lam, theta, H, B, X):
     for b, x in zip(B, X):
         v = matvec(desc, lam, 2, d * b)
         e = d * v - x
-        xx = float(x @ x)
-        loss += float(e @ e) / xx / K
+        if residual:
+            f = matvec(desc, lam, 0, e)
+            nn = float(b @ b)
+            loss += float(f @ f) / nn / K
+            e = matvec(desc, lam, 0, f)
+        else:
+            nn = float(x @ x)
+            loss += float(e @ e) / nn / K
         w = matvec(desc, lam, 2, d * e)
-        gcell += (2.0 / (xx * K)) * (e * v + b * w) * d
+        gcell += (2.0 / (nn * K)) * (e * v + b * w) * d
     gc = gcell.reshape(n[2], n[1], n[0])
     gprof = [gc.sum(axis=(0, 1)), gc.sum(axis=(0, 2)), gc.sum(axis=(1, 2))]
     w1, b1, w2 = theta[:H], theta[H:2 * H], theta[2 * H:3 * H]

@@ -1483,6 +1483,15 @@ pf_status pf_multiply_inverse(pf_plan* P, const double* b, double* x, int32_t me
   }
   pf_cg_report rep{};
   pf_status st = cg_solve(P, bd, xd, o, &rep);
+  if (st == PF_ERR_NOT_CONVERGED && P->learned && o.mode == PF_CG_RESIDUAL && o.precondition) {
+    // plain CG is the fallback of the learned preconditioner: solve again with P0 alone
+    pf_learned* keep = P->learned;
+    P->learned = nullptr;
+    const int used = rep.iterations;
+    st = cg_solve(P, bd, xd, o, &rep);
+    rep.iterations += used;
+    P->learned = keep;
+  }
   if (report) *report = rep;
   if (st != PF_OK && st != PF_ERR_NOT_CONVERGED) return check_bounds(P, st);
   if (mem != PF_MEM_DEVICE) CK(cudaMemcpyAsync(x, xd, bytes, cudaMemcpyDeviceToHost, P->stream));

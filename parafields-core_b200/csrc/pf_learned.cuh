@@ -13,10 +13,13 @@
 // (so it transfers across sizes and correlation lengths).  M is symmetric positive definite
 // for every parameter value, so plain preconditioned CG stays valid.
 //
-// Training fits M to (b, x = A^-1 b) pairs produced by plain CG:
-//     L = (1/count) sum_i ||D P0 D b_i - x_i||^2 / ||x_i||^2,
-//     dL/dd = (2/count) sum_i (e_i * v_i + b_i * P0(d * e_i)) / ||x_i||^2,
-// with v_i = P0(d * b_i) and e_i = d * v_i - x_i (P0 is symmetric); d = exp(sum psi) gives
+// Training fits M to (b, x = A^-1 b) pairs produced by plain CG, with e_i = M b_i - x_i
+// measured either in the solution norm or in the residual norm (A e_i = A M b_i - b_i, which
+// weighs every eigen-direction of A M alike, as the CG convergence does):
+//     L_sol = (1/count) sum_i ||e_i||^2 / ||x_i||^2,   L_res = (1/count) sum_i ||A e_i||^2 / ||b_i||^2,
+//     dL/dd = sum_i c_i (g_i * v_i + b_i * P0(d * g_i)),
+// with v_i = P0(d * b_i), g_i = e_i, c_i = 2/(count ||x_i||^2) (solution norm) or g_i = A A e_i,
+// c_i = 2/(count ||b_i||^2) (residual norm; P0 and A are symmetric); d = exp(sum psi) gives
 // dL/dpsi_i[m] = sum over the cells with coordinate m on axis i of d * dL/dd.
 // Parameters: theta = [w1(H), b1(H), w2(H), b2], psi(t) = sum_h w2_h tanh(w1_h t + b1_h) + b2.
 // Every reduction has a fixed order (deterministic training).
@@ -77,6 +80,31 @@ __global__ void __launch_bounds__(kLpThreads) k_lp_err(const double* __restrict_
   }
   s0[threadIdx.x] = a;
   s1[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = kLpThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      s0[threadIdx.x] += s0[threadIdx.x + w];
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = s0[0];
+    part[2 * blockIdx.x + 1] = s1[0];
+  }
+}
+
+// per-block partial sums of a.a and c.c (fixed grid: deterministic)
+__global__ void __launch_bounds__(kLpThreads) k_lp_sq2(const double* __restrict__ a, const double* __restrict__ c,
+                                                       uint64_t n, double* __restrict__ part) {
+  __shared__ double s0[kLpThreads], s1[kLpThreads];
+  double x = 0., y = 0.;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    x += a[i] * a[i];
+    y += c[i] * c[i];
+  }
+  s0[threadIdx.x] = x;
+  s1[threadIdx.x] = y;
   __syncthreads();
   for (int w = kLpThreads / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) {

@@ -175,6 +175,7 @@ def lib():
         "pf_learned_train": (i32, [vp, vp, vp, i32, i32, i32, C.c_double, i32, C.POINTER(C.c_double)]),
         "pf_learned_apply": (i32, [vp, vp, vp, i32]),
         "pf_plan_set_preconditioner": (i32, [vp, vp]),
+        "pf_learned_set_loss": (i32, [vp, i32]),
         "pf_last_error_string": (C.c_char_p, []),
         "pf_version": (C.c_char_p, []),
     }
@@ -371,10 +372,11 @@ class Ensemble:
 class Learned:
     """Learned boundary correction M = D P0 D of a plan's CG preconditioner."""
 
-    def __init__(self, plan, hidden=8, seed=0):
+    def __init__(self, plan, hidden=8, seed=0, residual_loss=False):
         h = C.c_void_p()
         _check(lib().pf_learned_create(plan.h, hidden, seed, C.byref(h)))
         self.h = h
+        _check(lib().pf_learned_set_loss(self.h, int(residual_loss)))
         self.plan = plan
         self.hidden = hidden
         self.n = int(lib().pf_learned_param_count(self.h))

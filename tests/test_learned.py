@@ -32,38 +32,41 @@ def _pairs(oracle, d, lam, K, seed):
     return B, X
 
 
+@pytest.mark.parametrize("residual", [False, True], ids=["solution-norm", "residual-norm"])
 @pytest.mark.parametrize("cfg", [CFG2, CFG3], ids=["2d-geo", "3d-axi"])
-def test_oracle_gradient_finite_differences(oracle, cfg):
+def test_oracle_gradient_finite_differences(oracle, cfg, residual):
     d = desc_of(cfg)
     lam, st, status = oracle.spectrum(d)
     assert (lam > 0).all()
     H = 4
     th = _theta(H, 1)
     B, X = _pairs(oracle, d, lam, 2, 2)
-    L, G = oracle.learned_loss_grad(d, lam, th, H, B, X)
+    L, G = oracle.learned_loss_grad(d, lam, th, H, B, X, residual)
     for p in range(len(th)):
         h = 1e-6 * max(1.0, abs(th[p]))
         tp, tm = th.copy(), th.copy()
         tp[p] += h
         tm[p] -= h
-        fd = (oracle.learned_loss_grad(d, lam, tp, H, B, X)[0] - oracle.learned_loss_grad(d, lam, tm, H, B, X)[0]) / (2 * h)
+        fd = (oracle.learned_loss_grad(d, lam, tp, H, B, X, residual)[0]
+              - oracle.learned_loss_grad(d, lam, tm, H, B, X, residual)[0]) / (2 * h)
         assert abs(fd - G[p]) <= 1e-6 * max(1.0, abs(G).max()), (p, fd, G[p])
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("residual", [False, True], ids=["solution-norm", "residual-norm"])
 @pytest.mark.parametrize("cfg", [CFG2, CFG3], ids=["2d-geo", "3d-axi"])
-def test_device_loss_and_gradient_match_oracle(oracle, cfg):
+def test_device_loss_and_gradient_match_oracle(oracle, cfg, residual):
     d = desc_of(cfg)
     P = pfb200.Plan(d)
     P.spectrum_build()
     lam, _, _ = oracle.spectrum(d)
     H = 6
-    Lp = pfb200.Learned(P, hidden=H, seed=3)
+    Lp = pfb200.Learned(P, hidden=H, seed=3, residual_loss=residual)
     th = _theta(H, 4)
     Lp.params = th
     B, X = _pairs(oracle, d, lam, 3, 5)
     loss, grad = Lp.loss_grad(B, X, fp32=False)
-    L0, G0 = oracle.learned_loss_grad(d, lam, th, H, B, X)
+    L0, G0 = oracle.learned_loss_grad(d, lam, th, H, B, X, residual)
     assert abs(loss - L0) <= 1e-10 * abs(L0)
     assert rel(grad, G0) < 1e-9
     # the learned application equals D P0 D on the oracle
