@@ -399,7 +399,7 @@ def run_cinv(args):
     Lp = pfb200.Learned(P, hidden=8, seed=11, residual_loss=args.residual_loss)
     loss0, _ = Lp.loss_grad(Bt, Xt, fp32=True)
     t0 = time.perf_counter()
-    loss1 = Lp.train(Bt, Xt, epochs=args.epochs, lr=0.05, fp32=True)
+    loss1 = Lp.train(Bt, Xt, epochs=args.epochs, lr=args.lr, fp32=True)
     ttrain = time.perf_counter() - t0
     Bs = torch.tensor(rng.standard_normal((K_test, N)), device="cuda")
     x = torch.empty(N, dtype=torch.float64, device="cuda")
@@ -424,7 +424,8 @@ def run_cinv(args):
                       "eigen": st, "plain": out["plain"], "learned": out["learned"],
                       "training": {"pairs": K_train, "pair_generation_s": tpairs, "epochs": args.epochs,
                                    "loss": "residual norm" if args.residual_loss else "solution norm",
-                                   "train_s": ttrain, "loss_before": loss0, "loss_after": loss1}}), flush=True)
+                                   "lr": args.lr, "train_s": ttrain, "loss_before": loss0,
+                                   "loss_after": loss1}}), flush=True)
     Lp.close()
 
 
@@ -470,6 +471,7 @@ def main():
     ap.add_argument("--train-pairs", type=int, default=16)
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--residual-loss", action="store_true")
+    ap.add_argument("--lr", type=float, default=0.005)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

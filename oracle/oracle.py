@@ -278,3 +278,61 @@ def learned_loss_grad(desc, lam, theta, H, B, X, residual=False):
         grad[H:2 * H] += gp @ dA
         grad[3 * H] += gp.sum()
     return loss, grad
+
+
+# ---------------------------------------------------------------------------
+# DCT/DST field backend (opt-in in the reference), FP64 restatement in numpy/scipy:
+# DCTDSTFieldBackend::setType / set / backwardTransform / extendedFieldToField
+# (include/parafields/backends/dctdstfieldbackend.hh:149-165, 326-438, 631-771) driven by
+# Matrix::generateField (include/parafields/matrix.hh:342-367).  scipy.fft.dct/dst of type 1
+# without normalization are FFTW's REDFT00/RODFT00.  fftw.transposed = false.
+# ---------------------------------------------------------------------------
+def dctdst_noise_size(desc):
+    dim = desc.dim
+    factor = 1 if desc.periodic else desc.embedding_factor
+    D = int(np.prod([factor * desc.cells[i] // 2 + 1 for i in range(dim)]))
+    return D << dim
+
+
+def generate_dctdst(desc, lam, noise):
+    """Field of the reference's DCT/DST backend for DCT eigenvalues `lam` (natural layout,
+    dim 0 fastest) and draws `noise` (type-major, then DCT cell index, dim 0 fastest).
+    The first type replaces the field (the documented intent; the reference's non-additive
+    extraction also adds, dctdstfieldbackend.hh:923)."""
+    import scipy.fft as sf
+    dim = desc.dim
+    factor = 1 if desc.periodic else desc.embedding_factor
+    n = [desc.cells[i] for i in range(dim)]
+    T = [factor * c for c in n]
+    D = [t // 2 + 1 for t in T]
+    shape = tuple(reversed(D))  # numpy order (d-1, ..., 0)
+    sq = np.sqrt(np.maximum(np.asarray(lam, dtype=np.float64), 0.0)).reshape(shape)
+    Dtot = int(np.prod(D))
+    field = np.zeros(tuple(reversed(n)))
+    for t in range(1 << dim):
+        odd = [(t >> i) & 1 for i in range(dim)]
+        r = np.asarray(noise[t * Dtot:(t + 1) * Dtot], dtype=np.float64).reshape(shape)
+        X = sq * r * 2.0 ** (-dim / 2.0)
+        for i in range(dim):
+            ax = dim - 1 - i
+            idx = [slice(None)] * dim
+            if odd[i]:
+                for e in (0, D[i] - 1):  # odd axis on its border: zero
+                    idx[ax] = e
+                    X[tuple(idx)] = 0.0
+            else:
+                for e in (0, D[i] - 1):  # even axis on its border: factor sqrt(2)
+                    idx[ax] = e
+                    X[tuple(idx)] *= np.sqrt(2.0)
+        for i in range(dim):
+            ax = dim - 1 - i
+            if odd[i]:
+                inner = [slice(None)] * dim
+                inner[ax] = slice(1, D[i] - 1)
+                Y = np.zeros_like(X)
+                Y[tuple(inner)] = sf.dst(X[tuple(inner)], type=1, axis=ax)
+                X = Y
+            else:
+                X = sf.dct(X, type=1, axis=ax)
+        field += X[tuple(slice(0, c) for c in reversed(n))]
+    return field.ravel()

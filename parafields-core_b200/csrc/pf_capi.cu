@@ -101,7 +101,10 @@ static pf_status resolve(const pf_field_desc* d, Geom* g) {
     return fail(PF_ERR_CONFIG, "dim 1 requires DFTMatrixBackend and DFTFieldBackend");
   if (fb == PF_FIELD_DFT && mb == PF_MATRIX_R2C)
     return fail(PF_ERR_CONFIG, "R2CMatrixBackend cannot serve DFTFieldBackend");
-  if (fb == PF_FIELD_DCTDST) return fail(PF_ERR_CONFIG, "DCTDSTFieldBackend is not supported");
+  // matrix.hh:342-347: the DCT/DST field backend needs the DCT matrix backend
+  if (fb == PF_FIELD_DCTDST && mb != PF_MATRIX_DCT) return fail(PF_ERR_CONFIG, "DCTDSTFieldBackend requires DCTMatrixBackend");
+  if (fb == PF_FIELD_DCTDST && d->dim > 1 && d->transposed != 0)
+    return fail(PF_ERR_CONFIG, "DCTDSTFieldBackend is supported with fftw.transposed = false only");
   for (int i = 0; i < d->dim; i++)
     if (mb == PF_MATRIX_DCT && (g->T[i] % 2))
       return fail(PF_ERR_CONFIG, "DCTMatrixBackend requires an even number of extended cells per dimension");
@@ -126,7 +129,9 @@ static pf_status resolve(const pf_field_desc* d, Geom* g) {
   }
   g->Nc = g->N / (uint64_t)g->T[0] * (uint64_t)g->T0c;
   g->S = mb == PF_MATRIX_DCT ? g->D : (mb == PF_MATRIX_R2C ? g->Nc : g->N);
-  g->noise = fb == PF_FIELD_R2C ? 2 * g->Nc : 2 * g->N;
+  // draws per realization: (rand1, rand2) per stored frequency, or one draw per DCT cell and
+  // symmetry type for DCTDSTFieldBackend (matrix.hh:349-366)
+  g->noise = fb == PF_FIELD_R2C ? 2 * g->Nc : (fb == PF_FIELD_DCTDST ? (g->D << d->dim) : 2 * g->N);
   for (int i = 0; i < 3; i++) g->C[i] = 1;
   for (int i = 0; i < d->dim; i++)
     g->C[i] = mb == PF_MATRIX_DCT ? g->T[i] / 2 + 1 : (mb == PF_MATRIX_R2C ? (i == 0 ? g->T0c : g->T[i]) : g->T[i]);
@@ -1082,6 +1087,63 @@ static pf_status gen_dft(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
                            (double)rows * (g.T[0] * e + 2.0 * g.n[0] * sizeof(S)));
 }
 
+// DCT/DST field backend (matrix.hh:342-367, dctdstfieldbackend.hh): for each of the 2^d
+// even/odd symmetry types, the scaled noise extended to the whole torus (DctDstNoise),
+// complex backward transforms along every axis and the real part added into the field
+template <typename T, typename S>
+static pf_status gen_dctdst(pf_plan* P, const double* noise_dev, uint64_t seed, S* out, int transform) {
+  const Geom& g = P->g;
+  DctDstNoise nz{};
+  nz.dim = g.dim;
+  for (int i = 0; i < 3; i++) {
+    nz.ext[i] = g.T[i];
+    nz.D[i] = i < g.dim ? g.T[i] / 2 + 1 : 1;
+  }
+  nz.sq = sizeof(T) == 8 ? (const void*)P->sq64 : (const void*)P->sq32;
+  nz.noise = noise_dev;
+  nz.seed = seed;
+  nz.nsq = (unsigned)g.S;
+  nz.nnoise = (unsigned)g.noise;
+  nz.Dtot = (unsigned)g.D;
+  const double e = sizeof(cx<T>);
+  const int last = g.dim - 1;
+  const long long inner = (long long)(g.N / (uint64_t)g.T[last]);
+  for (int type = 0; type < (1 << g.dim); type++) {
+    nz.type = type;
+    AccStore<S> as{out, g.n[0], type != 0, (unsigned)g.domain};
+    if (g.dim == 1) {
+      TRY(run_pass<T, true>(P, "gen_dctdst_d0", g.T[0], g.n[0], 1, 1, +1, +1, nz, NoMid(), as,
+                            (double)g.T[0] * (8.0 + sizeof(T)) + 2.0 * g.n[0] * sizeof(S)));
+      continue;
+    }
+    void *W1 = nullptr, *W2 = nullptr;
+    TRY(workspace(P, 0, sizeof(cx<T>) * (size_t)inner * g.n[last], &W1));
+    TRY(run_pass<T, false>(P, "gen_dctdst_noise", g.T[last], g.n[last], inner, 1, +1, +1, nz, NoMid(),
+                           arr_store<cx<T>>(P, W1, inner, 0, 1),
+                           (double)inner * (g.T[last] * (8.0 + sizeof(T)) + g.n[last] * e)));
+    void* cur = W1;
+    if (g.dim == 3) {
+      TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)g.T[0] * g.n[1] * g.n[2], &W2));
+      TRY((run_pass<T, false>(P, "gen_dctdst_d1", g.T[1], g.n[1], g.T[0], g.n[2], +1, +1,
+                              arr_load<cx<T>>(P, W1, g.T[0], (long long)g.T[0] * g.T[1], 1, g.T[1]), NoMid(),
+                              arr_store<cx<T>>(P, W2, g.T[0], (long long)g.T[0] * g.n[1], 1),
+                              (double)g.T[0] * g.n[2] * (g.T[1] + g.n[1]) * e)));
+      cur = W2;
+    }
+    const long long rows = g.dim == 3 ? (long long)g.n[1] * g.n[2] : g.n[1];
+    TRY(run_pass<T, true>(P, "gen_dctdst_d0", g.T[0], g.n[0], rows, 1, +1, +1,
+                          arr_load<cx<T>>(P, cur, 1, 0, g.T[0], g.T[0]), NoMid(), as,
+                          (double)rows * (g.T[0] * e + 2.0 * g.n[0] * sizeof(S))));
+  }
+  if (transform) {  // the value transform acts on the summed field (randomfield.hh:641-651)
+    ProfRec rec;
+    TRY(prof_begin(P, "transform", g.domain * 2.0 * sizeof(S), &rec));
+    k_transform<S><<<grid_for(g.domain), kThreads, 0, P->stream>>>(out, g.domain, transform, P->desc.boxcox_lambda);
+    TRY(prof_end(P, &rec));
+  }
+  return PF_OK;
+}
+
 // ---------------------------------------------------------------------------
 // matvecs: multiplyExtended / Root / InverseExtended (matrix.hh:1443-1646)
 // ---------------------------------------------------------------------------
@@ -1197,6 +1259,8 @@ static pf_status matvec_dft(pf_plan* P, int op, const S* in, S* out) {
 
 template <typename T, typename S>
 static pf_status matvec_dev(pf_plan* P, int op, const S* in, S* out) {
+  if (P->g.fb == PF_FIELD_DCTDST)
+    return fail(PF_ERR_CONFIG, "matrix-vector products with DCTDSTFieldBackend are not supported");
   if (P->g.fb == PF_FIELD_R2C) return matvec_r2c<T, S>(P, op, in, out);
   return matvec_dft<T, S>(P, op, in, out);
 }
@@ -1232,6 +1296,9 @@ static pf_status stage_noise(pf_plan* P, const double* noise, int noise_mem, con
 template <typename S>
 static pf_status generate_typed(pf_plan* P, const double* nd, uint64_t seed, S* out_dev, int transform) {
   const bool f64 = sizeof(S) == 8;
+  if (P->g.fb == PF_FIELD_DCTDST)
+    return f64 ? gen_dctdst<double, S>(P, nd, seed, out_dev, transform)
+               : gen_dctdst<float, S>(P, nd, seed, out_dev, transform);
   if (P->g.fb == PF_FIELD_R2C)
     return f64 ? gen_r2c<double, S>(P, nd, seed, out_dev, transform) : gen_r2c<float, S>(P, nd, seed, out_dev, transform);
   TRY(ensure(P, &P->spare, &P->spare_cap, P->g.domain * sizeof(S)));

@@ -348,6 +348,23 @@ struct SplitStore {
   }
 };
 
+// Re of a complex row into a real field, replacing (first symmetry type) or adding to the
+// field (later types): DCTDSTFieldBackend::extendedFieldToField with `additive`
+// (dctdstfieldbackend.hh:631-771)
+template <typename S>
+struct AccStore {
+  S* out;
+  int n0;
+  int accumulate;
+  unsigned n;
+  template <typename T>
+  __device__ __forceinline__ void store(long long p, int j, long long, cx<T> v) const {
+    const unsigned i = (unsigned)p * (unsigned)n0 + (unsigned)j;
+    if (!in_bounds32(i, n)) return;
+    out[i] = accumulate ? (S)(out[i] + (S)v.x) : (S)v.x;
+  }
+};
+
 // complex row load of a real field (DFT backend embedding, dftfieldbackend.hh:307-325)
 template <typename S>
 struct FieldComplexLoad {
@@ -812,6 +829,80 @@ struct DFTNoise {
       normal_pair<T>(seed, si, r1, r2);
     }
     return mk<T>(lam * r1, lam * r2);
+  }
+};
+
+// Noise of one even/odd symmetry type of the DCT/DST field backend, extended to the whole
+// torus so that complex backward transforms along every axis reproduce the mixed
+// REDFT00/RODFT00 transform of the reference (dctdstfieldbackend.hh:149-165, 326-438):
+//  - stored value at DCT index m (m_i <= T_i/2): 2^{-d/2} sqrt(lambda(m)) r 2^{b/2}, b = number
+//    of even axes with m_i on the border (0 or T_i/2), and 0 if an odd axis is on its border
+//    (DCTDSTFieldBackend::set, 418-438); r is draw type*D + flat(m) of the reference order;
+//  - torus frequency k maps to m_i = min(k_i, T_i - k_i), with the sign -1 on odd axes for
+//    k_i > T_i/2: then sum_k x(k) e^{+2 pi i k.x/T} = i^{#odd} * (REDFT00 x RODFT00 ...)(x),
+//    since sum over an odd axis gives 2i sum sin(pi m x / (T/2)) = i RODFT00;
+//  - the loader multiplies by i^{-#odd}, so the real part of the transform is the reference's
+//    field of this type.
+// Pencils of the first pass run along the last axis: p enumerates (k0, k1), j is k_last.
+struct DctDstNoise {
+  int dim;
+  int ext[3];
+  int D[3];
+  int type;  // bit i set: axis i odd (RODFT00)
+  const void* sq;
+  const double* noise;
+  uint64_t seed;
+  unsigned nsq, nnoise;
+  unsigned Dtot;
+  template <typename T>
+  __device__ __forceinline__ cx<T> load(long long p, int j, long long) const {
+    int k[3] = {0, 0, 0};
+    if (dim == 1) {
+      k[0] = j;
+    } else if (dim == 2) {
+      k[0] = (int)p;
+      k[1] = j;
+    } else {
+      k[0] = (int)(p % ext[0]);
+      k[1] = (int)(p / ext[0]);
+      k[2] = j;
+    }
+    int m[3] = {0, 0, 0};
+    int sign = 1, border = 0, nodd = 0;
+    for (int i = 0; i < dim; i++) {
+      const int h = ext[i] / 2;
+      m[i] = k[i] <= h ? k[i] : ext[i] - k[i];
+      const bool edge = m[i] == 0 || m[i] == h;
+      if ((type >> i) & 1) {
+        if (edge) return mk<T>(0, 0);
+        if (k[i] > h) sign = -sign;
+        nodd++;
+      } else if (edge) {
+        border++;
+      }
+    }
+    const unsigned li = (unsigned)m[0] + (unsigned)D[0] * ((unsigned)m[1] + (unsigned)D[1] * (unsigned)m[2]);
+    if (!in_bounds32(li, nsq)) return mk<T>(0, 0);
+    const unsigned ri = (unsigned)type * Dtot + li;
+    T r;
+    if (noise) {
+      if (!in_bounds32(ri, nnoise)) return mk<T>(0, 0);
+      r = (T)noise[ri];
+    } else {
+      T r2;
+      normal_pair<T>(seed, ri, r, r2);
+    }
+    T v = ((const T*)sq)[li] * r * (T)sign;
+    // 2^{-d/2} 2^{b/2}
+    const int e = border - dim;
+    v *= (e & 1) ? (T)0.70710678118654752440084436210484903928 : (T)1;
+    v = ldexp(v, (e + (e & 1)) / 2);
+    switch (nodd & 3) {
+      case 0: return mk<T>(v, 0);
+      case 1: return mk<T>(0, -v);
+      case 2: return mk<T>(-v, 0);
+      default: return mk<T>(0, v);
+    }
   }
 };
 

@@ -381,3 +381,63 @@ def test_ensemble_device_replay_is_new_noise(oracle):
     assert not torch.equal(a, b)
     assert abs(float(a.std()) - float(b.std())) < 0.2 * float(a.std())
     E.close()
+
+
+# ---------------------------------------------------------------------------
+# DCT/DST field backend (opt-in in the reference; fftw.transposed = false)
+# ---------------------------------------------------------------------------
+DCTDST = {
+    "2d-exp-iso": dict(dim=2, cells=(40, 36), covariance="exponential", corr_length=0.1),
+    "2d-m52-axi-pow2": dict(dim=2, cells=(128, 64), covariance="matern52", corr_length=(0.1, 0.05),
+                            anisotropy="axiparallel", approximate=True),
+    "3d-sph-iso": dict(dim=3, cells=(20, 16, 12), covariance="spherical", corr_length=0.2),
+}
+
+
+def _dctdst_descs(cfg, prec, **extra):
+    over = dict(transposed=0, precision=prec, matrix_backend=pfb200.MATRIX_DCT, **extra)
+    return (desc_of(cfg, field_backend=pfb200.FIELD_DCTDST, **over),
+            desc_of(cfg, field_backend=pfb200.FIELD_R2C, **over))
+
+
+@pytest.mark.parametrize("prec", [pfb200.PREC_F64, pfb200.PREC_F32])
+@pytest.mark.parametrize("name", list(DCTDST))
+def test_dctdst_generate_parity(oracle, name, prec):
+    d, dr = _dctdst_descs(DCTDST[name], prec, transform="logNormal")
+    lam, st, _ = oracle.spectrum(dr)
+    P = pfb200.Plan(d)
+    P.spectrum_build()
+    assert P.info.noise_size == oracle.dctdst_noise_size(d)
+    noise = oracle.noise(20261203, P.info.noise_size)
+    tol = TOL64F if prec == pfb200.PREC_F64 else TOL32
+    ref = oracle.generate_dctdst(d, lam, noise)
+    assert rel(P.generate(noise=noise), ref) < tol
+    # the value transform acts on the summed field of all symmetry types
+    assert rel(P.generate(noise=noise, apply_transform=True), np.exp(ref)) < tol
+    P.close()
+
+
+def test_dctdst_seeded_covariance(oracle):
+    """Seeded DCT/DST realizations: empirical covariance against the exact covariance of the
+    circulant embedding (which the DCT/DST generator reproduces exactly)."""
+    cfg = dict(dim=2, cells=(8, 6), covariance="exponential", corr_length=0.3)
+    d, dr = _dctdst_descs(cfg, pfb200.PREC_F64)
+    lam, _, _ = oracle.spectrum(dr)
+    g = oracle.resolve(dr)
+    C = np.stack([oracle.matvec(dr, lam, pfb200.OP_MUL, np.eye(g.domain)[j]) for j in range(g.domain)], axis=1) * g.N
+    P = pfb200.Plan(d)
+    M = 20000
+    fields = P.generate_batch(seed=99, count=M).reshape(M, g.domain)
+    emp = fields.T @ fields / M
+    se = np.sqrt((np.diag(C)[:, None] * np.diag(C)[None, :] + C ** 2) / M)
+    assert (np.abs(emp - C) < 5 * se + 1e-12).mean() > 0.995
+    P.close()
+
+
+def test_dctdst_rejects_matvec_and_transposed():
+    d = desc_of(DCTDST["2d-exp-iso"], transposed=0, field_backend=pfb200.FIELD_DCTDST)
+    P = pfb200.Plan(d)
+    with pytest.raises(pfb200.PfError):
+        P.matvec(np.zeros(P.info.domain_size))
+    with pytest.raises(pfb200.PfError):
+        pfb200.Plan(desc_of(DCTDST["2d-exp-iso"], field_backend=pfb200.FIELD_DCTDST))

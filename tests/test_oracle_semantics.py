@@ -181,3 +181,22 @@ def test_general_matern_matches_closed_forms(oracle, nu):
     a = desc_of(dict(dim=2, cells=(16, 12), covariance="matern", matern_nu=nu, corr_length=ell))
     b = desc_of(dict(dim=2, cells=(16, 12), covariance=closed, corr_length=ell))
     np.testing.assert_allclose(oracle.fill_matrix(a), oracle.fill_matrix(b), rtol=1e-12, atol=1e-15)
+
+
+def test_dctdst_oracle_covariance_equals_circulant_embedding(oracle):
+    """The DCT/DST restatement reproduces the embedded covariance: summing the 2^d symmetry
+    types, the exact covariance J J^T of its generator equals the torus covariance restricted
+    to the domain (circulant embedding without the R2C half-spectrum quirk)."""
+    import pfb200
+    d = pfb200.make_desc(dim=2, cells=(6, 5), covariance="exponential", corr_length=0.3, transposed=0,
+                         field_backend=pfb200.FIELD_DCTDST)
+    dr = pfb200.make_desc(dim=2, cells=(6, 5), covariance="exponential", corr_length=0.3, transposed=0)
+    lam, st, _ = oracle.spectrum(dr)
+    m = oracle.dctdst_noise_size(d)
+    J = np.stack([oracle.generate_dctdst(d, lam, np.eye(m)[i]) for i in range(m)], axis=1)
+    cov = J @ J.T
+    # torus covariance between domain cells, from the unit-vector matvec (returns C e_j / N)
+    g = oracle.resolve(dr)
+    C = np.stack([oracle.matvec(dr, lam, pfb200.OP_MUL, np.eye(g.domain)[j]) for j in range(g.domain)], axis=1)
+    C *= g.N
+    assert np.abs(cov - C).max() < 1e-12 * np.abs(C).max()
