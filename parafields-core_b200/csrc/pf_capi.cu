@@ -218,6 +218,11 @@ struct pf_plan {
   bool borrowed_ws = false;
   // learned preconditioner of the residual-mode CG (pf_plan_set_preconditioner), not owned
   pf_learned* learned = nullptr;
+  // pipelined batches: two streams, each with its own pair of generation workspaces
+  cudaStream_t lane[2] = {nullptr, nullptr};
+  cudaEvent_t lane_ev[3] = {nullptr, nullptr, nullptr};
+  void* ws_b[2] = {nullptr, nullptr};
+  size_t ws_b_bytes[2] = {0, 0};
 };
 
 static pf_status dalloc(pf_plan* P, void** p, size_t bytes) {
@@ -1381,6 +1386,12 @@ void pf_plan_destroy(pf_plan* P) {
     cudaEventDestroy(r.e1);
   }
   for (auto e : P->evpool) cudaEventDestroy(e);
+  for (int l = 0; l < 2; l++) {
+    if (P->ws_b[l]) cudaFree(P->ws_b[l]);
+    if (P->lane[l]) cudaStreamDestroy(P->lane[l]);
+  }
+  for (int l = 0; l < 3; l++)
+    if (P->lane_ev[l]) cudaEventDestroy(P->lane_ev[l]);
   if (P->own) cudaStreamDestroy(P->own);
   delete P;
 }
@@ -1479,6 +1490,44 @@ pf_status pf_generate_batch(pf_plan* P, uint64_t seed, int32_t count, void* out,
   const size_t es = P->desc.precision == PF_PREC_F64 ? 8 : 4;
   const size_t bytes = P->g.domain * es;
   const int tr = apply_transform ? P->desc.transform : 0;
+  if (P->g.fb == PF_FIELD_R2C && out_mem == PF_MEM_DEVICE && count >= 2) {
+    // Realizations are independent: alternate them over two streams, each with its own
+    // workspaces, so that one realization's issue-bound noise pass overlaps the other's
+    // memory-bound passes.  The caller's stream waits for both at the end.
+    if (!P->lane[0])
+      for (int l = 0; l < 2; l++)
+        CK(cudaStreamCreateWithFlags(&P->lane[l], cudaStreamNonBlocking));
+    if (!P->lane_ev[0])
+      for (int l = 0; l < 3; l++) CK(cudaEventCreateWithFlags(&P->lane_ev[l], cudaEventDisableTiming));
+    cudaStream_t caller = P->stream;
+    CK(cudaEventRecord(P->lane_ev[0], caller));
+    for (int l = 0; l < 2; l++) CK(cudaStreamWaitEvent(P->lane[l], P->lane_ev[0], 0));
+    pf_status st = PF_OK;
+    for (int32_t r = 0; r < count && st == PF_OK; r++) {
+      const int slot = r & 1;
+      void* dst = (char*)out + (size_t)r * bytes;
+      if (slot)
+        for (int i = 0; i < 2; i++) {
+          std::swap(P->ws[i], P->ws_b[i]);
+          std::swap(P->ws_bytes[i], P->ws_b_bytes[i]);
+        }
+      P->stream = P->lane[slot];
+      st = es == 8 ? gen_r2c<double, double>(P, nullptr, seed + r, (double*)dst, tr)
+                   : gen_r2c<float, float>(P, nullptr, seed + r, (float*)dst, tr);
+      P->stream = caller;
+      if (slot)
+        for (int i = 0; i < 2; i++) {
+          std::swap(P->ws[i], P->ws_b[i]);
+          std::swap(P->ws_bytes[i], P->ws_b_bytes[i]);
+        }
+    }
+    for (int l = 0; l < 2; l++) {
+      CK(cudaEventRecord(P->lane_ev[1 + l], P->lane[l]));
+      CK(cudaStreamWaitEvent(caller, P->lane_ev[1 + l], 0));
+    }
+    P->spare_valid = false;
+    return check_bounds(P, st);
+  }
   for (int32_t r = 0; r < count; r++) {
     void* dst = (char*)out + (size_t)r * bytes;
     if (out_mem != PF_MEM_DEVICE) {

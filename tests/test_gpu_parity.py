@@ -441,3 +441,20 @@ def test_dctdst_rejects_matvec_and_transposed():
         P.matvec(np.zeros(P.info.domain_size))
     with pytest.raises(pfb200.PfError):
         pfb200.Plan(desc_of(DCTDST["2d-exp-iso"], field_backend=pfb200.FIELD_DCTDST))
+
+
+@pytest.mark.parametrize("name", ["3d-matern32-axi-pow2", "2d-exp-prime"])
+def test_pipelined_batch_equals_single_calls(name):
+    """pf_generate_batch with device output alternates realizations over two streams with
+    separate workspaces; every realization equals the one-at-a-time call with its seed."""
+    torch = pytest.importorskip("torch")
+    P = pfb200.Plan(desc_of(CONFIGS[name], precision=pfb200.PREC_F32))
+    n = P.info.domain_size
+    batch = torch.empty(5 * n, dtype=torch.float32, device="cuda")
+    P.generate_batch(seed=41, count=5, out=batch)
+    one = torch.empty(n, dtype=torch.float32, device="cuda")
+    for r in range(5):
+        P.generate(seed=41 + r, out=one)
+        torch.cuda.synchronize()
+        assert torch.equal(batch[r * n:(r + 1) * n], one), r
+    P.close()
