@@ -333,6 +333,20 @@ pf_status pf_learned_apply(pf_learned* learned, const double* r, double* z, int3
 /* Attaches `learned` (NULL detaches) as the preconditioner of PF_CG_RESIDUAL solves of `plan`. */
 pf_status pf_plan_set_preconditioner(pf_plan* plan, pf_learned* learned);
 
+/* Measured planning, the counterpart of fftw.measure / fftw.useWisdom (r2cfieldbackend.hh:
+ * 212-230, fieldtraits.hh:175-186): times every candidate of each realization pass of the
+ * plan (paired-FP32 or scalar kernels x resident CTAs per SM of the persistent kernels,
+ * `repetitions` realizations each, default 3) and keeps the fastest per pass.  Choices go to
+ * a process-wide wisdom table keyed by the pass geometry; a plan whose passes are all in it
+ * takes them without timing (*timed = 0).  Clears the plan's profiling records.  R2C field
+ * backend only (other plans: no-op). */
+pf_status pf_plan_autotune(pf_plan* plan, int32_t repetitions, int32_t* timed);
+/* Wisdom as text, one line "pass L pencils outer precision variant ctas_per_sm" per entry;
+ * *needed = bytes including the terminating NUL. */
+pf_status pf_wisdom_export(char* buf, uint64_t cap, uint64_t* needed);
+pf_status pf_wisdom_import(const char* text);
+void pf_wisdom_forget(void);
+
 /* ValueTransform::apply (mutators.hh:35-163) over `count` values of `precision`. */
 pf_status pf_apply_transform(pf_plan* plan, int32_t precision, void* data, uint64_t count,
                              int32_t mem);

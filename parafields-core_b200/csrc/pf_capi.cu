@@ -218,6 +218,12 @@ struct pf_plan {
   bool borrowed_ws = false;
   // learned preconditioner of the residual-mode CG (pf_plan_set_preconditioner), not owned
   pf_learned* learned = nullptr;
+  // autotuned choices per generation pass (0 noise, 1 middle c2c, 2 c2r): kernel family
+  // (0: paired FP32 where eligible, 1: scalar) and resident CTAs per SM of persistent
+  // kernels (0: as many as fit); grid_cap is the value of the pass being launched
+  int tune_variant[3] = {0, 0, 0};
+  int tune_grid[3] = {0, 0, 0};
+  int grid_cap = 0;
   // pipelined batches: two streams, each with its own pair of generation workspaces
   cudaStream_t lane[2] = {nullptr, nullptr};
   cudaEvent_t lane_ev[3] = {nullptr, nullptr, nullptr};
@@ -526,6 +532,7 @@ static pf_status persistent_grid(pf_plan* P, K kern, size_t smem, long long ntil
   int per = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kThreads, smem));
   if (per < 1) per = 1;
+  if (P->grid_cap > 0 && P->grid_cap < per) per = P->grid_cap;
   long long g = (long long)per * sm_count(P);
   if (g > ntiles) g = ntiles;
   *grid = (unsigned)(g > 0 ? g : 1);
@@ -997,7 +1004,12 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
   const long long jst = g.dim == 3 ? (long long)P0 * g.T[1] : P0;
   const double b1 = (double)T0c * outer * (Tl * (noise_b + lam_b) + (double)g.n[last] * e);
   constexpr bool F32 = std::is_same<T, float>::value && std::is_same<S, float>::value;
-  if (F32 && p2_length(Tl) && p2_view_ok(W1, jst, P0, outer))
+  struct CapReset {
+    pf_plan* P;
+    ~CapReset() { P->grid_cap = 0; }
+  } cap_reset{P};
+  P->grid_cap = P->tune_grid[0];
+  if (F32 && P->tune_variant[0] == 0 && p2_length(Tl) && p2_view_ok(W1, jst, P0, outer))
     TRY(p2_noise(P, "gen_noise_last", Tl, g.n[last], T0c, outer, nz, p2_store(P, W1, jst, P0, T0c), b1));
   else if (Tl % 2 == 0)
     TRY((run_fpass<T, +1, +1, false, true>(P, "gen_noise_last", Tl, g.n[last], T0c, outer, nz, NoMid(),
@@ -1010,7 +1022,8 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
     void* W2 = nullptr;
     TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)P0 * g.n[1] * g.n[2], &W2));
     const double b2 = (double)T0c * g.n[2] * (g.T[1] + g.n[1]) * e;
-    if (F32 && p2_length(g.T[1]) && p2_view_ok(W1, P0, (long long)P0 * g.T[1], g.n[2]) &&
+    P->grid_cap = P->tune_grid[1];
+    if (F32 && P->tune_variant[1] == 0 && p2_length(g.T[1]) && p2_view_ok(W1, P0, (long long)P0 * g.T[1], g.n[2]) &&
         p2_view_ok(W2, P0, (long long)P0 * g.n[1], g.n[2]))
       TRY(p2_c2c<+1>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, g.n[2],
                      p2_load(P, W1, P0, (long long)P0 * g.T[1], g.T[1], T0c),
@@ -1024,8 +1037,9 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
   }
   const long long rows = g.dim == 3 ? (long long)g.n[1] * g.n[2] : g.n[1];
   const double b3 = (double)rows * (T0c * e + g.n[0] * sizeof(S));
+  P->grid_cap = P->tune_grid[2];
   if constexpr (F32) {
-    if (g.T[0] % 2 == 0 && p2_length(g.T[0] / 2)) {
+    if (P->tune_variant[2] == 0 && g.T[0] % 2 == 0 && p2_length(g.T[0] / 2)) {
       P2RowLoad rl;
       rl.ptr = (const float2*)cur;
       rl.rowstride = (unsigned)P0;
@@ -1838,3 +1852,4 @@ extern "C" pf_status pf_matvec_static(pf_plan* P, int32_t op, const double* in, 
 }
 
 #include "pf_ensemble.inc"
+#include "pf_tune.inc"

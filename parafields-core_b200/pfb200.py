@@ -176,6 +176,10 @@ def lib():
         "pf_learned_apply": (i32, [vp, vp, vp, i32]),
         "pf_plan_set_preconditioner": (i32, [vp, vp]),
         "pf_learned_set_loss": (i32, [vp, i32]),
+        "pf_plan_autotune": (i32, [vp, i32, C.POINTER(i32)]),
+        "pf_wisdom_export": (i32, [C.c_char_p, u64, C.POINTER(u64)]),
+        "pf_wisdom_import": (i32, [C.c_char_p]),
+        "pf_wisdom_forget": (None, []),
         "pf_last_error_string": (C.c_char_p, []),
         "pf_version": (C.c_char_p, []),
     }
@@ -313,6 +317,13 @@ class Plan:
         return [{"name": arr[i].name.decode(), "launches": arr[i].launches,
                  "total_ms": arr[i].total_ms, "bytes": arr[i].bytes} for i in range(n.value)]
 
+    def autotune(self, repetitions=3):
+        """Measured planning of the realization passes; True if it timed candidates (False
+        when every pass came from the wisdom table)."""
+        t = C.c_int32()
+        _check(lib().pf_plan_autotune(self.h, repetitions, C.byref(t)))
+        return bool(t.value)
+
     def launch_count(self):
         return int(lib().pf_launch_count(self.h))
 
@@ -430,3 +441,19 @@ class Learned:
             self.close()
         except Exception:
             pass
+
+
+def wisdom_export():
+    need = C.c_uint64()
+    _check(lib().pf_wisdom_export(None, 0, C.byref(need)))
+    buf = C.create_string_buffer(int(need.value))
+    _check(lib().pf_wisdom_export(buf, need.value, C.byref(need)))
+    return buf.value.decode()
+
+
+def wisdom_import(text):
+    _check(lib().pf_wisdom_import(text.encode()))
+
+
+def wisdom_forget():
+    lib().pf_wisdom_forget()

@@ -458,3 +458,28 @@ def test_pipelined_batch_equals_single_calls(name):
         torch.cuda.synchronize()
         assert torch.equal(batch[r * n:(r + 1) * n], one), r
     P.close()
+
+
+@pytest.mark.parametrize("name", ["3d-matern32-axi-pow2", "2d-exp-prime"])
+def test_autotune_and_wisdom(oracle, name):
+    """Measured planning changes only kernel choices: parity holds after it; the wisdom it
+    records serves a second plan without timing, also after an export/import round trip."""
+    pfb200.wisdom_forget()
+    d, P, lam, st, _ = plan_and_oracle(oracle, CONFIGS[name], precision=pfb200.PREC_F32)
+    g = oracle.resolve(d)
+    noise = oracle.noise(7, g.noise)
+    ref, _ = oracle.generate(d, lam, noise)
+    assert P.autotune(repetitions=2) is True
+    assert rel(P.generate(noise=noise), ref) < TOL32
+    text = pfb200.wisdom_export()
+    assert len(text.strip().splitlines()) == g.dim
+    P2 = pfb200.Plan(d)
+    assert P2.autotune() is False
+    pfb200.wisdom_forget()
+    pfb200.wisdom_import(text)
+    P3 = pfb200.Plan(d)
+    assert P3.autotune() is False
+    assert rel(P3.generate(noise=noise), ref) < TOL32
+    pfb200.wisdom_forget()
+    for Q in (P, P2, P3):
+        Q.close()
