@@ -148,7 +148,26 @@ typedef struct pf_field_desc {
   int32_t cg_iterations;     /* randomField.cgIterations (default 100) */
   int32_t transform;         /* pf_transform, randomField.transform */
   double boxcox_lambda;      /* transform.boxCoxLambda */
+  /* smooth periodization (matrix.hh:510-602, 652-775): */
+  int32_t periodization;     /* pf_periodization, embedding.periodization */
+  int32_t sigmoid;           /* pf_sigmoid, embedding.sigmoid */
+  int32_t sigmoid_combine;   /* pf_sigmoid_combine, stochastic.sigmoidCombine */
+  int32_t merge_recursions;  /* embedding.mergeRecursions (99: the covariance's default) */
+  double sigmoid_start;      /* embedding.sigmoidStart (default 1) */
+  double sigmoid_end;        /* embedding.sigmoidEnd (negative: default factor - 1) */
 } pf_field_desc;
+
+/* embedding.periodization: classical mirroring or sigmoid merging of the 2^d mirrored
+ * copies (fold and cofold, which need GSL quadrature, are not built) */
+typedef enum pf_periodization { PF_PERIODIZATION_CLASSICAL = 0, PF_PERIODIZATION_MERGE = 1 } pf_periodization;
+/* embedding.sigmoid (covariance.hh:147-287) */
+typedef enum pf_sigmoid { PF_SIGMOID_SMOOTHSTEP = 0, PF_SIGMOID_SMOOTH = 1 } pf_sigmoid;
+/* stochastic.sigmoidCombine (matrix.hh:668-677) */
+typedef enum pf_sigmoid_combine {
+  PF_COMBINE_RADIAL_PLUS = 0,
+  PF_COMBINE_RADIAL = 1,
+  PF_COMBINE_TENSOR = 2
+} pf_sigmoid_combine;
 
 /* Eigenvalue statistics of matrix.hh:270-299 (counts and minimum). */
 typedef struct pf_eig_stats {

@@ -126,6 +126,12 @@ int oc_resolve(const pf_field_desc* d, oc_geom* g, char* err, int errlen) {
   if (d->covariance == PF_COV_CUBIC && d->dim == 3) FAIL("cubic covariance only applicable in 1D or 2D");
   if (d->anisotropy < 0 || d->anisotropy > 2)
     FAIL("stochastic.anisotropy must be \"none\", \"axiparallel\" or \"geometric\"");
+  /* matrix.hh:515-579 */
+  if (d->periodization < 0 || d->periodization > 1) FAIL("embedding.periodization must be classical or merge");
+  if (d->periodization == PF_PERIODIZATION_MERGE) {
+    if (d->sigmoid < 0 || d->sigmoid > 1) FAIL("embedding.sigmoid must be \"smooth\" or \"smoothstep\"");
+    if (d->sigmoid_combine < 0 || d->sigmoid_combine > 2) FAIL("sigmoidCombine must be tensor, radial or radialPlus");
+  }
 #undef FAIL
   return PF_OK;
 }
@@ -706,6 +712,93 @@ static void fill_cells(const oc_geom* g, int* cells) {
   }
 }
 
+/* ClampingSigmoid / SmoothstepSigmoid / SmoothSigmoid (covariance.hh:147-287) */
+static double oc_sigmoid(int kind, double oneEdge, double zeroEdge, double x, unsigned int recursions) {
+  if (kind == PF_SIGMOID_SMOOTH) {
+    if (fabs(x) < oneEdge) return 1.;
+    if (fabs(x) > zeroEdge) return 0.;
+    const double x1 = (zeroEdge - fabs(x)) / (zeroEdge - oneEdge);
+    const double x2 = (fabs(x) - oneEdge) / (zeroEdge - oneEdge);
+    const double th1 = x1 > 0. ? exp(-1. / x1) : 0.;
+    const double th2 = x2 > 0. ? exp(-1. / x2) : 0.;
+    return th1 / (th1 + th2);
+  }
+  double x1;
+  if (fabs(x) < oneEdge)
+    x1 = 1.;
+  else if (fabs(x) > zeroEdge)
+    x1 = 0.;
+  else
+    x1 = (zeroEdge - fabs(x)) / (zeroEdge - oneEdge);
+  const double x2 = 2. * x1 - 1.;
+  double normalization = 1., addition = 1., output = 1.;
+  for (unsigned int i = 1; i <= recursions; i++) {
+    output *= 2. * i;
+    addition *= 1 - x2 * x2;
+    output += addition;
+    output /= 2. * i + 1.;
+    normalization *= 2. * i / (2. * i + 1.);
+  }
+  output *= x2 / normalization;
+  output += 1.;
+  output /= 2.;
+  return output;
+}
+
+/* mergeRecursions default 99 (matrix.hh:693-717) */
+static unsigned int oc_merge_recursions(const pf_field_desc* d) {
+  if (d->merge_recursions != 99) return (unsigned int)d->merge_recursions;
+  switch (d->covariance) {
+    case PF_COV_MATERN: return (unsigned int)floor(d->matern_nu * 2. + d->dim / 2.);
+    case PF_COV_GAMMA_EXPONENTIAL: return (unsigned int)floor(d->exp_gamma + d->dim / 2.);
+    case PF_COV_GENERALIZED_CAUCHY: return (unsigned int)floor(d->cauchy_alpha + d->dim / 2.);
+    case PF_COV_EXPONENTIAL: return 2;
+    case PF_COV_MATERN32: return 4;
+    case PF_COV_MATERN52: return 6;
+    case PF_COV_CAUCHY: return 3;
+    default: return 0;
+  }
+}
+
+/* computeMatrixEntriesWithMerge (matrix.hh:652-775) at true coordinates tc */
+static double oc_merge_value(const pf_field_desc* d, const oc_geom* g, const double* tc) {
+  const int dim = g->dim;
+  const unsigned int factor = (unsigned int)g->factor;
+  const double start = d->sigmoid_start;
+  const double end = d->sigmoid_end < 0 ? (double)factor - 1. : d->sigmoid_end;
+  const unsigned int rec = oc_merge_recursions(d);
+  const int radial = d->sigmoid_combine != PF_COMBINE_TENSOR;
+  double constValue = 0.;
+  if (d->sigmoid_combine == PF_COMBINE_RADIAL_PLUS) {
+    double half[3] = {0, 0, 0}, th[3] = {0, 0, 0};
+    for (int i = 0; i < dim; i++) half[i] = g->ext[i] * factor / 2.;
+    oc_geometry(d, half, th);
+    constValue = oc_covariance(d, th);
+  }
+  const double eps = 1e-10;
+  const double sqrtDim = sqrt((double)dim);
+  double value = 0., remainder = 1.;
+  for (unsigned int j = 0; j < (1u << dim); j++) {
+    double mirror[3] = {0, 0, 0}, trans[3] = {0, 0, 0};
+    for (int i = 0; i < dim; i++) mirror[i] = (j & (1u << i)) ? g->ext[i] * factor - tc[i] : tc[i];
+    double dampening = 1.;
+    if (radial && sqrtDim < factor / 2.) {
+      double radius = 0.;
+      for (int i = 0; i < dim; i++) radius += (mirror[i] * mirror[i]) / (g->ext[i] * g->ext[i]);
+      radius = sqrt(radius);
+      dampening = oc_sigmoid(d->sigmoid, start * sqrtDim - eps, factor - (factor - end) * sqrtDim + eps, radius, rec);
+    } else {
+      for (int i = 0; i < dim; i++)
+        dampening *= oc_sigmoid(d->sigmoid, g->ext[i] * start - eps, g->ext[i] * end + eps, mirror[i], rec);
+    }
+    if (dampening < eps) continue;
+    remainder -= dampening;
+    oc_geometry(d, mirror, trans);
+    value += oc_covariance(d, trans) * dampening;
+  }
+  return value + constValue * remainder;
+}
+
 int oc_fill_matrix(const pf_field_desc* d, double* out, uint64_t count) {
   oc_geom g;
   int st = oc_resolve(d, &g, NULL, 0);
@@ -719,6 +812,15 @@ int oc_fill_matrix(const pf_field_desc* d, double* out, uint64_t count) {
   for (long long idx = 0; idx < (long long)total; idx++) {
     long long r = idx;
     double coord[3] = {0, 0, 0}, tc[3] = {0, 0, 0};
+    if (d->periodization == PF_PERIODIZATION_MERGE) {
+      for (int i = 0; i < g.dim; i++) {
+        unsigned int ii = (unsigned int)(r % cells[i]);
+        r /= cells[i];
+        coord[i] = (double)ii * g.h[i];
+      }
+      out[idx] = oc_merge_value(d, &g, coord);
+      continue;
+    }
     for (int i = 0; i < g.dim; i++) {
       unsigned int ii = (unsigned int)(r % cells[i]);
       r /= cells[i];

@@ -149,6 +149,18 @@ static pf_status resolve(const pf_field_desc* d, Geom* g) {
   if (c == PF_COV_CUBIC && d->dim == 3) return fail(PF_ERR_CONFIG, "cubic covariance only applicable in 1D or 2D");
   if (d->anisotropy < 0 || d->anisotropy > 2)
     return fail(PF_ERR_CONFIG, "stochastic.anisotropy must be \"none\", \"axiparallel\" or \"geometric\"");
+  if (d->periodization < 0 || d->periodization > 1)
+    return fail(PF_ERR_CONFIG, "embedding.periodization must be \"classical\" or \"merge\" (fold and cofold are not built)");
+  if (d->periodization == PF_PERIODIZATION_MERGE) {
+    if (d->sigmoid < 0 || d->sigmoid > 1)
+      return fail(PF_ERR_CONFIG, "embedding.sigmoid must be \"smooth\" or \"smoothstep\"");
+    if (d->sigmoid_combine < 0 || d->sigmoid_combine > 2)
+      return fail(PF_ERR_CONFIG, "sigmoidCombine must be tensor, radial or radialPlus");
+    if (d->merge_recursions == 99 && c != PF_COV_MATERN && c != PF_COV_GAMMA_EXPONENTIAL &&
+        c != PF_COV_GENERALIZED_CAUCHY && c != PF_COV_EXPONENTIAL && c != PF_COV_MATERN32 &&
+        c != PF_COV_MATERN52 && c != PF_COV_CAUCHY)
+      return fail(PF_ERR_CONFIG, "magic recursions value 99 not implemented for choice of covariance");
+  }
   if (d->precision != PF_PREC_F64 && d->precision != PF_PREC_F32) return fail(PF_ERR_CONFIG, "unknown precision");
   return PF_OK;
 }
@@ -762,6 +774,29 @@ static CovParams cov_params(const pf_field_desc* d, const Geom& g) {
     c.p2 = std::tgamma(d->matern_nu);
     c.p3 = d->matern_nu;
   }
+  c.per = d->periodization;
+  c.sig = d->sigmoid;
+  c.radial = d->sigmoid_combine != PF_COMBINE_TENSOR;
+  c.plus = d->sigmoid_combine == PF_COMBINE_RADIAL_PLUS;
+  c.factor = (double)g.factor;
+  c.sstart = d->sigmoid_start;
+  c.send = d->sigmoid_end < 0 ? (double)g.factor - 1. : d->sigmoid_end;
+  for (int i = 0; i < 3; i++) c.ext[i] = g.ext[i];
+  int rec = d->merge_recursions;
+  if (rec == 99) {  // matrix.hh:693-717
+    const double hd = (double)g.dim / 2.;
+    switch (d->covariance) {
+      case PF_COV_MATERN: rec = (int)std::floor(d->matern_nu * 2. + hd); break;
+      case PF_COV_GAMMA_EXPONENTIAL: rec = (int)std::floor(d->exp_gamma + hd); break;
+      case PF_COV_GENERALIZED_CAUCHY: rec = (int)std::floor(d->cauchy_alpha + hd); break;
+      case PF_COV_EXPONENTIAL: rec = 2; break;
+      case PF_COV_MATERN32: rec = 4; break;
+      case PF_COV_MATERN52: rec = 6; break;
+      case PF_COV_CAUCHY: rec = 3; break;
+      default: rec = 0;
+    }
+  }
+  c.rec = rec;
   return c;
 }
 
@@ -1357,6 +1392,12 @@ void pf_field_desc_init(pf_field_desc* d) {
   d->eigen_check = PF_EIGCHECK_CORRECTED;
   d->cg_iterations = 100;
   d->transform = PF_TRANSFORM_NONE;
+  d->periodization = PF_PERIODIZATION_CLASSICAL;
+  d->sigmoid = PF_SIGMOID_SMOOTHSTEP;
+  d->sigmoid_combine = PF_COMBINE_RADIAL_PLUS;
+  d->merge_recursions = 99;
+  d->sigmoid_start = 1.0;
+  d->sigmoid_end = -1.0;
 }
 
 pf_status pf_plan_create(const pf_field_desc* desc, pf_plan** plan) {

@@ -395,6 +395,14 @@ struct CovParams {
   double variance;
   double p0, p1;    // gamma / alpha / beta; matern: sqrt(2 nu), 2^(1-nu)
   double p2, p3;    // matern: Gamma(nu), nu
+  // merge periodization (matrix.hh:652-775)
+  int per;          // 0 classical mirroring, 1 merge
+  int sig;          // 0 smoothstep, 1 smooth
+  int radial;       // radial or radialPlus combination of the sigmoids
+  int plus;         // radialPlus: remainder filled with the covariance at half the torus
+  int rec;          // sigmoid recursions
+  double sstart, send, factor;
+  double ext[3];
 };
 
 // Modified Bessel function of the second kind K_nu(x), nu >= 0, x > 0.
@@ -551,9 +559,93 @@ __device__ __forceinline__ double cov_eval(const CovParams& c, const double* xt)
   }
 }
 
-// covariance at torus cell (j0, j1, j2) with the classical mirroring
+// GeometryMatrix::transform (covariance.hh:18-138)
+__device__ __forceinline__ void geo_apply(const CovParams& c, const double* x, double* xt) {
+  if (c.aniso == 0) {
+    for (int i = 0; i < c.dim; i++) xt[i] = c.geo[0] * x[i];
+  } else if (c.aniso == 1) {
+    for (int i = 0; i < c.dim; i++) xt[i] = c.geo[i] * x[i];
+  } else {
+    for (int i = 0; i < c.dim; i++) {
+      double s = 0.;
+      for (int k = 0; k < c.dim; k++) s += c.geo[i * c.dim + k] * x[k];
+      xt[i] = s;
+    }
+  }
+}
+
+// SmoothstepSigmoid over ClampingSigmoid (covariance.hh:204-287)
+__device__ __forceinline__ double sigmoid_smoothstep(double one, double zero, double x, int rec) {
+  const double ax = fabs(x);
+  const double x1 = ax < one ? 1. : (ax > zero ? 0. : (zero - ax) / (zero - one));
+  const double x2 = 2. * x1 - 1.;
+  double normalization = 1., addition = 1., output = 1.;
+  for (int i = 1; i <= rec; i++) {
+    output *= 2. * i;
+    addition *= 1 - x2 * x2;
+    output += addition;
+    output /= 2. * i + 1.;
+    normalization *= 2. * i / (2. * i + 1.);
+  }
+  output *= x2 / normalization;
+  output += 1.;
+  output /= 2.;
+  return output;
+}
+
+// SmoothSigmoid (covariance.hh:147-195)
+__device__ __forceinline__ double sigmoid_smooth(double one, double zero, double x) {
+  const double ax = fabs(x);
+  if (ax < one) return 1.;
+  if (ax > zero) return 0.;
+  const double x1 = (zero - ax) / (zero - one), x2 = (ax - one) / (zero - one);
+  const double t1 = x1 > 0. ? exp(-1. / x1) : 0., t2 = x2 > 0. ? exp(-1. / x2) : 0.;
+  return t1 / (t1 + t2);
+}
+
+__device__ __forceinline__ double sigmoid_of(const CovParams& c, double one, double zero, double x) {
+  return c.sig ? sigmoid_smooth(one, zero, x) : sigmoid_smoothstep(one, zero, x, c.rec);
+}
+
+// computeMatrixEntriesWithMerge (matrix.hh:652-775) at torus cell jj: the 2^d mirrored
+// copies of the covariance, each damped by the sigmoid, plus the remainder times the
+// covariance at half the torus (radialPlus)
+__device__ __noinline__ double cov_merge(const CovParams& c, const int* jj) {
+  double tc[3] = {0, 0, 0}, mc[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
+  for (int i = 0; i < c.dim; i++) tc[i] = (double)(unsigned int)jj[i] * c.h[i];
+  double cst = 0.;
+  if (c.plus) {
+    for (int i = 0; i < c.dim; i++) mc[i] = c.ext[i] * c.factor / 2.;
+    geo_apply(c, mc, xt);
+    cst = cov_eval(c, xt);
+  }
+  const double eps = 1e-10;
+  const double sqrtDim = sqrt((double)c.dim);
+  double value = 0., remainder = 1.;
+  for (int m = 0; m < (1 << c.dim); m++) {
+    for (int i = 0; i < c.dim; i++) mc[i] = ((m >> i) & 1) ? c.ext[i] * c.factor - tc[i] : tc[i];
+    double damp = 1.;
+    if (c.radial && sqrtDim < c.factor / 2.) {
+      double radius = 0.;
+      for (int i = 0; i < c.dim; i++) radius += (mc[i] * mc[i]) / (c.ext[i] * c.ext[i]);
+      radius = sqrt(radius);
+      damp = sigmoid_of(c, c.sstart * sqrtDim - eps, c.factor - (c.factor - c.send) * sqrtDim + eps, radius);
+    } else {
+      for (int i = 0; i < c.dim; i++)
+        damp *= sigmoid_of(c, c.ext[i] * c.sstart - eps, c.ext[i] * c.send + eps, mc[i]);
+    }
+    if (damp < eps) continue;
+    remainder -= damp;
+    geo_apply(c, mc, xt);
+    value += cov_eval(c, xt) * damp;
+  }
+  return value + cst * remainder;
+}
+
+// covariance at torus cell (j0, j1, j2) with the classical mirroring (or the merge)
 __device__ __forceinline__ double cov_at(const CovParams& c, int j0, int j1, int j2) {
   const int jj[3] = {j0, j1, j2};
+  if (c.per == 1) return cov_merge(c, jj);
   double x[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
   for (int i = 0; i < c.dim; i++) {
     double v = (double)(unsigned int)jj[i] * c.h[i];

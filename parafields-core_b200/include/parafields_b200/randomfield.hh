@@ -96,8 +96,30 @@ pf_field_desc descFromConfig(const ParameterTree& config) {
   d.threshold = config.get<double>("embedding.threshold", 1e-14);
   if (config.hasKey("fftw.transposed")) d.transposed = config.get<bool>("fftw.transposed") ? 1 : 0;
   const std::string per = config.get<std::string>("embedding.periodization", std::string("classical"));
-  if (per != "classical")
+  if (per == "merge") {
+    d.periodization = PF_PERIODIZATION_MERGE;
+    const std::string sig = config.get<std::string>("embedding.sigmoid", std::string("smoothstep"));
+    if (sig == "smooth")
+      d.sigmoid = PF_SIGMOID_SMOOTH;
+    else if (sig == "smoothstep")
+      d.sigmoid = PF_SIGMOID_SMOOTHSTEP;
+    else
+      throw std::runtime_error{"embedding.sigmoid must be \"smooth\" or \"smoothstep\""};
+    const std::string comb = config.get<std::string>("stochastic.sigmoidCombine", std::string("radialPlus"));
+    if (comb == "radialPlus")
+      d.sigmoid_combine = PF_COMBINE_RADIAL_PLUS;
+    else if (comb == "radial")
+      d.sigmoid_combine = PF_COMBINE_RADIAL;
+    else if (comb == "tensor")
+      d.sigmoid_combine = PF_COMBINE_TENSOR;
+    else
+      throw std::runtime_error{"sigmoidCombine must be tensor, radial or radialPlus"};
+    d.sigmoid_start = config.get<double>("embedding.sigmoidStart", 1.);
+    d.sigmoid_end = config.get<double>("embedding.sigmoidEnd", (double)d.embedding_factor - 1.);
+    d.merge_recursions = (int32_t)config.get<unsigned>("embedding.mergeRecursions", 99u);
+  } else if (per != "classical") {
     throw std::runtime_error{"embedding.periodization \"" + per + "\" is not available on the B200 path"};
+  }
   const std::string optim = config.get<std::string>("embedding.optim", std::string("none"));
   if (optim != "none") throw std::runtime_error{"optimization requires dune-nonlinopt"};
   const std::string tr = config.get<std::string>("randomField.transform", std::string("none"));

@@ -30,6 +30,9 @@ COVARIANCES = {
 }
 ANISOTROPIES = {"none": 0, "axiparallel": 1, "geometric": 2}
 TRANSFORMS = {"none": 0, "logNormal": 1, "foldedNormal": 2, "sign": 3, "boxCox": 4}
+PERIODIZATIONS = {"classical": 0, "merge": 1}
+SIGMOIDS = {"smoothstep": 0, "smooth": 1}
+COMBINES = {"radialPlus": 0, "radial": 1, "tensor": 2}
 MATRIX_DCT, MATRIX_R2C, MATRIX_DFT = 0, 1, 2
 FIELD_R2C, FIELD_DFT, FIELD_DCTDST = 0, 1, 2
 PREC_F64, PREC_F32 = 0, 1
@@ -49,6 +52,8 @@ class FieldDesc(C.Structure):
         ("transposed", C.c_int32), ("matrix_backend", C.c_int32), ("field_backend", C.c_int32),
         ("precision", C.c_int32), ("eigen_check", C.c_int32), ("cg_iterations", C.c_int32),
         ("transform", C.c_int32), ("boxcox_lambda", C.c_double),
+        ("periodization", C.c_int32), ("sigmoid", C.c_int32), ("sigmoid_combine", C.c_int32),
+        ("merge_recursions", C.c_int32), ("sigmoid_start", C.c_double), ("sigmoid_end", C.c_double),
     ]
 
 
@@ -90,7 +95,9 @@ def make_desc(dim=2, cells=(16, 16), extensions=None, covariance="exponential", 
               approximate=False, threshold=1e-14, transposed=-1, matrix_backend=-1,
               field_backend=-1, precision=PREC_F64, eigen_check=EIGCHECK_CORRECTED,
               cg_iterations=100, transform="none", boxcox_lambda=0.0, matern_nu=0.5,
-              exp_gamma=1.0, cauchy_alpha=1.0, cauchy_beta=1.0) -> FieldDesc:
+              exp_gamma=1.0, cauchy_alpha=1.0, cauchy_beta=1.0, periodization="classical",
+              sigmoid="smoothstep", sigmoid_combine="radialPlus", merge_recursions=99,
+              sigmoid_start=1.0, sigmoid_end=-1.0) -> FieldDesc:
     """Builds a descriptor from values named after the reference's config keys."""
     d = FieldDesc()
     d.dim = dim
@@ -126,6 +133,11 @@ def make_desc(dim=2, cells=(16, 16), extensions=None, covariance="exponential", 
     d.cg_iterations = cg_iterations
     d.transform = TRANSFORMS[transform] if isinstance(transform, str) else int(transform)
     d.boxcox_lambda = boxcox_lambda
+    d.periodization = PERIODIZATIONS[periodization] if isinstance(periodization, str) else int(periodization)
+    d.sigmoid = SIGMOIDS[sigmoid] if isinstance(sigmoid, str) else int(sigmoid)
+    d.sigmoid_combine = COMBINES[sigmoid_combine] if isinstance(sigmoid_combine, str) else int(sigmoid_combine)
+    d.merge_recursions = merge_recursions
+    d.sigmoid_start, d.sigmoid_end = sigmoid_start, sigmoid_end
     return d
 
 

@@ -47,6 +47,17 @@ CONFIGS = {
                             anisotropy="geometric", approximate=True),
     "3d-exp-iso-notransp-pow2": dict(dim=3, cells=(64, 64, 128), covariance="exponential", corr_length=0.05,
                                      transposed=0),
+    # merge periodization (matrix.hh:652-775): radial branch needs sqrt(dim) < factor/2
+    "2d-merge-radialplus-f3": dict(dim=2, cells=(48, 40), covariance="matern32", corr_length=0.3,
+                                   embedding_factor=3, periodization="merge", sigmoid_start=1.0,
+                                   sigmoid_end=2.0, approximate=True),
+    "3d-merge-tensor-smooth": dict(dim=3, cells=(16, 16, 12), covariance="exponential", corr_length=0.2,
+                                   periodization="merge", sigmoid="smooth", sigmoid_combine="tensor",
+                                   sigmoid_start=0.7, sigmoid_end=1.0, approximate=True),
+    "2d-merge-radial-geo-f4": dict(dim=2, cells=(32, 24), covariance="exponential",
+                                   corr_length=(0.2, 0.05, -0.05, 0.15), anisotropy="geometric",
+                                   embedding_factor=4, periodization="merge", sigmoid_combine="radial",
+                                   sigmoid_start=1.0, sigmoid_end=3.0, approximate=True),
     # tori whose lengths have prime factors above 13: Bluestein transforms
     "2d-exp-prime": dict(dim=2, cells=(131, 97), covariance="exponential", corr_length=0.1),
     "3d-sph-prime": dict(dim=3, cells=(17, 19, 23), covariance="spherical", corr_length=0.2),

@@ -208,3 +208,34 @@ def test_host_philox_known_answer():
     from test_gpu_parity import _philox4x32_10
     z = np.zeros(1, dtype=np.uint64)
     assert [int(v[0]) for v in _philox4x32_10((z, z, z, z), 0)] == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+
+
+def test_merge_periodization_with_default_sigmoid_edges_is_classical(oracle):
+    """embedding.periodization = merge with sigmoidStart 1 and sigmoidEnd = factor - 1 at
+    factor 2 is a step at the domain extent: the merged torus covariance equals the classical
+    mirroring (the two mirrors share the midpoint with weight 1/2 each)."""
+    import pfb200
+    for kw in (dict(dim=2, cells=(12, 10), covariance="matern32", corr_length=(0.2, 0.1)),
+               dict(dim=3, cells=(6, 8, 4), covariance="exponential", corr_length=0.15)):
+        for sig in ("smoothstep", "smooth"):
+            base = pfb200.make_desc(**kw)
+            merged = pfb200.make_desc(**kw, periodization="merge", sigmoid=sig)
+            a, b = oracle.fill_matrix(base), oracle.fill_matrix(merged)
+            assert np.abs(a - b).max() <= 1e-13 * np.abs(a).max()
+
+
+def test_merge_periodization_smooths_the_embedding(oracle):
+    """With factor 3 and a sigmoid transition between one and two extents, the merged
+    covariance keeps the prescribed values on the domain (distances below one extent) and
+    differs from the classical embedding in the transition zone."""
+    import pfb200
+    kw = dict(dim=2, cells=(16, 12), covariance="exponential", corr_length=0.5, embedding_factor=3)
+    base = pfb200.make_desc(**kw)
+    merged = pfb200.make_desc(**kw, periodization="merge", sigmoid_start=1.0, sigmoid_end=2.0,
+                              sigmoid_combine="tensor")
+    g = oracle.resolve(base)
+    a = oracle.fill_matrix(base).reshape(g.T[1] // 2 + 1, g.T[0] // 2 + 1)
+    b = oracle.fill_matrix(merged).reshape(g.T[1] // 2 + 1, g.T[0] // 2 + 1)
+    inside = (np.arange(g.T[1] // 2 + 1)[:, None] < g.n[1]) & (np.arange(g.T[0] // 2 + 1)[None, :] < g.n[0])
+    assert np.abs(a[inside] - b[inside]).max() < 1e-12
+    assert np.abs(a[~inside] - b[~inside]).max() > 1e-6
