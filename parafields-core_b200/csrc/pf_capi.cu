@@ -1545,10 +1545,11 @@ pf_status pf_generate_batch(pf_plan* P, uint64_t seed, int32_t count, void* out,
   const size_t es = P->desc.precision == PF_PREC_F64 ? 8 : 4;
   const size_t bytes = P->g.domain * es;
   const int tr = apply_transform ? P->desc.transform : 0;
-  if (P->g.fb == PF_FIELD_R2C && out_mem == PF_MEM_DEVICE && count >= 2) {
+  if (P->g.fb == PF_FIELD_R2C && count >= 2) {
     // Realizations are independent: alternate them over two streams, each with its own
     // workspaces, so that one realization's issue-bound noise pass overlaps the other's
-    // memory-bound passes.  The caller's stream waits for both at the end.
+    // memory-bound passes (and, for host output, the other's copy to the host, which runs
+    // asynchronously when `out` is pinned).  The caller's stream waits for both at the end.
     if (!P->lane[0])
       for (int l = 0; l < 2; l++)
         CK(cudaStreamCreateWithFlags(&P->lane[l], cudaStreamNonBlocking));
@@ -1557,10 +1558,15 @@ pf_status pf_generate_batch(pf_plan* P, uint64_t seed, int32_t count, void* out,
     cudaStream_t caller = P->stream;
     CK(cudaEventRecord(P->lane_ev[0], caller));
     for (int l = 0; l < 2; l++) CK(cudaStreamWaitEvent(P->lane[l], P->lane_ev[0], 0));
+    const bool host = out_mem != PF_MEM_DEVICE;
+    if (host) {  // one device staging buffer per stream
+      TRY(ensure(P, &P->io_dev, &P->io_cap, bytes));
+      TRY(ensure(P, &P->io2_dev, &P->io2_cap, bytes));
+    }
     pf_status st = PF_OK;
     for (int32_t r = 0; r < count && st == PF_OK; r++) {
       const int slot = r & 1;
-      void* dst = (char*)out + (size_t)r * bytes;
+      void* dst = host ? (slot ? P->io2_dev : P->io_dev) : (char*)out + (size_t)r * bytes;
       if (slot)
         for (int i = 0; i < 2; i++) {
           std::swap(P->ws[i], P->ws_b[i]);
@@ -1569,6 +1575,10 @@ pf_status pf_generate_batch(pf_plan* P, uint64_t seed, int32_t count, void* out,
       P->stream = P->lane[slot];
       st = es == 8 ? gen_r2c<double, double>(P, nullptr, seed + r, (double*)dst, tr)
                    : gen_r2c<float, float>(P, nullptr, seed + r, (float*)dst, tr);
+      if (st == PF_OK && host &&
+          cudaMemcpyAsync((char*)out + (size_t)r * bytes, dst, bytes, cudaMemcpyDeviceToHost, P->lane[slot]) !=
+              cudaSuccess)
+        st = fail(PF_ERR_CUDA, "copy of realization %d to the host failed", (int)r);
       P->stream = caller;
       if (slot)
         for (int i = 0; i < 2; i++) {

@@ -264,8 +264,100 @@ class RandomField {
   std::vector<RF> invMatvecPart_, invRootMatvecPart_;
   std::array<unsigned, dim> cells_;
   std::array<double, dim> ext_;
+  std::array<unsigned, dim> dataCells_;  // resolution of data_ and the cached parts
+  bool custom_ = false;
 
   void ensureMatrix() const {}
+
+  // StochasticPart::refine (stochastic.hh:597-672): each cell value copied to its 2^d children
+  std::vector<RF> refined(const std::vector<RF>& old) const {
+    static_assert(dim == 2 || dim == 3, "refine is implemented for dim 2 and 3, as in the reference");
+    std::array<unsigned, 3> n{1, 1, 1}, o{1, 1, 1};
+    for (unsigned i = 0; i < dim; i++) {
+      n[i] = cells_[i];
+      o[i] = dataCells_[i];
+    }
+    std::vector<RF> out((std::size_t)n[0] * n[1] * n[2]);
+    for (unsigned z = 0; z < n[2]; z++)
+      for (unsigned y = 0; y < n[1]; y++)
+        for (unsigned x = 0; x < n[0]; x++)
+          out[x + (std::size_t)n[0] * (y + (std::size_t)n[1] * z)] =
+              old[x / 2 + (std::size_t)o[0] * (y / 2 + (std::size_t)o[1] * (dim == 3 ? z / 2 : 0))];
+    return out;
+  }
+
+  // StochasticPart::coarsen (stochastic.hh:679-755): mean of the 2^d children, summed in the
+  // reference's order
+  std::vector<RF> coarsened(const std::vector<RF>& old) const {
+    static_assert(dim == 2 || dim == 3, "coarsen is implemented for dim 2 and 3, as in the reference");
+    std::array<unsigned, 3> n{1, 1, 1}, o{1, 1, 1};
+    for (unsigned i = 0; i < dim; i++) {
+      n[i] = cells_[i];
+      o[i] = dataCells_[i];
+    }
+    std::vector<RF> out((std::size_t)n[0] * n[1] * n[2]);
+    const std::size_t sx = 1, sy = o[0], sz = (std::size_t)o[0] * o[1];
+    for (unsigned z = 0; z < n[2]; z++)
+      for (unsigned y = 0; y < n[1]; y++)
+        for (unsigned x = 0; x < n[0]; x++) {
+          const std::size_t b = 2 * x + sy * (2 * y + (std::size_t)o[1] * (dim == 3 ? 2 * z : 0));
+          RF v = 0.;
+          v += old[b];
+          v += old[b + sx];
+          v += old[b + sy];
+          v += old[b + sy + sx];
+          if (dim == 3) {
+            v += old[b + sz];
+            v += old[b + sz + sx];
+            v += old[b + sz + sy];
+            v += old[b + sz + sy + sx];
+          }
+          out[x + (std::size_t)n[0] * (y + (std::size_t)n[1] * z)] = v / (RF)(1u << dim);
+        }
+    return out;
+  }
+
+  // RandomFieldTraits::refine / coarsen (fieldtraits.hh:321-348) + Matrix::update
+  void resizeMatrix(unsigned mul, unsigned div) {
+    for (unsigned i = 0; i < dim; i++) {
+      cells_[i] = cells_[i] * mul / div;
+      desc_.cells[i] = (int32_t)cells_[i];
+    }
+    matrix_ = std::make_shared<GpuMatrix<RF>>(desc_, custom_);
+  }
+
+  // RandomField::refine / coarsen (randomfield.hh:880-1018), using the cached matrix-vector
+  // products when they are valid
+  void changeLevel(bool up) {
+    if (dataCells_ == cells_) return;  // StochasticPart: level unchanged
+    const RF scale = std::pow(RF(0.5), up ? -RF(dim) : RF(dim));
+    auto level = [&](const std::vector<RF>& v) { return up ? refined(v) : coarsened(v); };
+    if (cacheInvMatvec_ && invMatvecValid_) {
+      invMatvecPart_ = level(invMatvecPart_);
+      matrix_->multiply(PF_OP_MUL, invMatvecPart_, data_);
+      for (auto& v : data_) v *= scale;
+      for (auto& v : invMatvecPart_) v *= scale;
+      if (cacheInvRootMatvec_) {
+        matrix_->multiply(PF_OP_ROOT, invMatvecPart_, invRootMatvecPart_);
+        for (auto& v : invRootMatvecPart_) v *= scale;
+        invRootMatvecValid_ = true;
+      }
+    } else if (cacheInvRootMatvec_ && invRootMatvecValid_) {
+      invRootMatvecPart_ = level(invRootMatvecPart_);
+      matrix_->multiply(PF_OP_ROOT, invRootMatvecPart_, data_);
+      for (auto& v : data_) v *= scale;
+      for (auto& v : invRootMatvecPart_) v *= scale;
+      if (cacheInvMatvec_) {
+        invMatvecPart_ = data_;
+        invMatvecValid_ = false;
+      }
+    } else {
+      data_ = level(data_);
+      if (cacheInvMatvec_) invMatvecPart_ = level(invMatvecPart_);
+      if (cacheInvRootMatvec_) invRootMatvecPart_ = level(invRootMatvecPart_);
+    }
+    dataCells_ = cells_;
+  }
 
  public:
   explicit RandomField(const ParameterTree& config)
@@ -275,8 +367,10 @@ class RandomField {
         cacheInvRootMatvec_(config.get<bool>("randomField.cacheInvRootMatvec", false)) {
     transform_ = ValueTransform<RF>(desc_.transform, (RF)desc_.boxcox_lambda);
     const std::string cov = config.get<std::string>("stochastic.covariance");
-    matrix_ = std::make_shared<GpuMatrix<RF>>(desc_, cov == "custom-iso" || cov == "custom-aniso");
+    custom_ = cov == "custom-iso" || cov == "custom-aniso";
+    matrix_ = std::make_shared<GpuMatrix<RF>>(desc_, custom_);
     cells_ = config.get<std::array<unsigned, dim>>("grid.cells");
+    dataCells_ = cells_;
     ext_ = config.get<std::array<double, dim>>("grid.extensions");
     data_.assign(matrix_->info().domain_size, RF(0));
     if (cacheInvMatvec_) invMatvecPart_ = data_;
@@ -284,6 +378,14 @@ class RandomField {
   }
 
   GpuMatrix<RF>& matrix() { return *matrix_; }
+
+  // randomfield.hh:880-887 / 955-961: double (halve) the resolution of the matrix
+  void refineMatrix() { resizeMatrix(2, 1); }
+  void coarsenMatrix() { resizeMatrix(1, 2); }
+  // randomfield.hh:897-945 / 971-1018: bring the field (and cached products) to the
+  // matrix's resolution
+  void refine() { changeLevel(true); }
+  void coarsen() { changeLevel(false); }
   const std::vector<RF>& dataVector() const { return data_; }
   std::vector<RF>& dataVector() { return data_; }
 

@@ -2,6 +2,8 @@
 //   facade_main config <ini>                 prints the descriptor built from the keys
 //   facade_main run <ini> <seed> <outdir>    generate / timesMatrix / timesInverseMatrix,
 //                                            writing noise, fields and products as raw doubles
+//   facade_main refine <ini> <seed> <outdir> refine / coarsen, without and with a cached
+//                                            inverse product (randomField.cacheInvMatvec)
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -44,6 +46,33 @@ static int run(const ParameterTree& cfg, unsigned seed, const std::string& out) 
   return 0;
 }
 
+template <unsigned dim>
+static int refine_run(const ParameterTree& cfg, unsigned seed, const std::string& out) {
+  if constexpr (dim == 1) {
+    return 5;
+  } else {
+    RandomField<dim> field(cfg);
+    field.generate(seed);
+    dump(out + "/field.bin", field.dataVector());
+    field.refineMatrix();
+    field.refine();
+    dump(out + "/refined.bin", field.dataVector());
+    field.coarsenMatrix();
+    field.coarsen();
+    dump(out + "/back.bin", field.dataVector());
+    // with the inverse product cached: timesMatrix keeps x, refine recomputes C_fine refine(x)
+    ParameterTree c2 = cfg;
+    c2["randomField.cacheInvMatvec"] = "true";
+    RandomField<dim> cached(c2);
+    cached.generate(seed);
+    cached.timesMatrix();
+    cached.refineMatrix();
+    cached.refine();
+    dump(out + "/cached_refined.bin", cached.dataVector());
+    return 0;
+  }
+}
+
 int main(int argc, char** argv) {
   if (argc < 3) return 2;
   ParameterTree cfg;
@@ -69,6 +98,7 @@ int main(int argc, char** argv) {
       return 0;
     }
     const unsigned seed = (unsigned)std::stoul(argv[3]);
+    if (mode == "refine") return dim == 2 ? refine_run<2>(cfg, seed, argv[4]) : refine_run<3>(cfg, seed, argv[4]);
     if (dim == 1) return run<1>(cfg, seed, argv[4]);
     if (dim == 2) return run<2>(cfg, seed, argv[4]);
     return run<3>(cfg, seed, argv[4]);

@@ -96,3 +96,23 @@ def test_facade_generate_and_products(facade_exe, tmp_path, oracle, dim):
     assert rel(ld("cinvcx.bin"), field) < 1e-6  # C^-1 (C x) = x up to the CG stopping rule
     w = ld("white.bin")
     assert abs(w.mean()) < 0.2 and abs(w.std() - 1) < 0.2
+
+
+@pytest.mark.gpu
+def test_facade_refine_coarsen(facade_exe, tmp_path, oracle):
+    """refineMatrix + refine copies every value to its 2^d children; coarsenMatrix + coarsen
+    averages them back; with randomField.cacheInvMatvec the refined C x is recomputed as
+    2^d C_fine refine(x) from the cached x (randomfield.hh:880-945)."""
+    ini = write_ini(tmp_path, "grid.cells = 24 20\ngrid.extensions = 1 1\nstochastic.corrLength = 0.1\n"
+                    "stochastic.variance = 1\nstochastic.covariance = exponential\n")
+    r = subprocess.run([facade_exe, "refine", ini, "5", str(tmp_path)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    ld = lambda n: np.fromfile(str(tmp_path / n), dtype=np.float64)
+    x = ld("field.bin").reshape(20, 24)
+    fine = np.repeat(np.repeat(x, 2, axis=0), 2, axis=1)
+    assert np.array_equal(ld("refined.bin").reshape(40, 48), fine)
+    assert np.allclose(ld("back.bin").reshape(20, 24), x, rtol=0, atol=1e-15)
+    d_fine = desc_of(dict(dim=2, cells=(48, 40), covariance="exponential", corr_length=0.1))
+    lam, _, _ = oracle.spectrum(d_fine)
+    ref = 4.0 * oracle.matvec(d_fine, lam, pfb200.OP_MUL, fine.ravel())
+    assert rel(ld("cached_refined.bin"), ref) < 1e-12

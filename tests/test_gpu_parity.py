@@ -494,3 +494,15 @@ def test_autotune_and_wisdom(oracle, name):
     pfb200.wisdom_forget()
     for Q in (P, P2, P3):
         Q.close()
+
+
+def test_pipelined_batch_to_host_equals_device_batch():
+    torch = pytest.importorskip("torch")
+    P = pfb200.Plan(desc_of(CONFIGS["3d-matern32-axi-pow2"], precision=pfb200.PREC_F32))
+    n = P.info.domain_size
+    dev = torch.empty(4 * n, dtype=torch.float32, device="cuda")
+    P.generate_batch(seed=9, count=4, out=dev)
+    host = torch.empty(4 * n, dtype=torch.float32).pin_memory().numpy()
+    P.generate_batch(seed=9, count=4, out=host)
+    assert np.array_equal(host, dev.cpu().numpy())
+    P.close()
