@@ -148,18 +148,25 @@ typedef struct pf_field_desc {
   int32_t cg_iterations;     /* randomField.cgIterations (default 100) */
   int32_t transform;         /* pf_transform, randomField.transform */
   double boxcox_lambda;      /* transform.boxCoxLambda */
-  /* smooth periodization (matrix.hh:510-602, 652-775): */
+  /* smooth periodization (matrix.hh:510-602, 652-890): */
   int32_t periodization;     /* pf_periodization, embedding.periodization */
   int32_t sigmoid;           /* pf_sigmoid, embedding.sigmoid */
   int32_t sigmoid_combine;   /* pf_sigmoid_combine, stochastic.sigmoidCombine */
   int32_t merge_recursions;  /* embedding.mergeRecursions (99: the covariance's default) */
   double sigmoid_start;      /* embedding.sigmoidStart (default 1) */
   double sigmoid_end;        /* embedding.sigmoidEnd (negative: default factor - 1) */
+  double fold_max_factor;    /* embedding.foldMaxFactor (default 1) */
+  int32_t fold_recursions;   /* embedding.foldRecursions (99: the covariance's default) */
+  int32_t pad_;
 } pf_field_desc;
 
-/* embedding.periodization: classical mirroring or sigmoid merging of the 2^d mirrored
- * copies (fold and cofold, which need GSL quadrature, are not built) */
-typedef enum pf_periodization { PF_PERIODIZATION_CLASSICAL = 0, PF_PERIODIZATION_MERGE = 1 } pf_periodization;
+/* embedding.periodization: classical mirroring, sigmoid merging of the 2^d mirrored copies,
+ * or folding of the distances beyond the domain (cofold is not built) */
+typedef enum pf_periodization {
+  PF_PERIODIZATION_CLASSICAL = 0,
+  PF_PERIODIZATION_MERGE = 1,
+  PF_PERIODIZATION_FOLD = 2
+} pf_periodization;
 /* embedding.sigmoid (covariance.hh:147-287) */
 typedef enum pf_sigmoid { PF_SIGMOID_SMOOTHSTEP = 0, PF_SIGMOID_SMOOTH = 1 } pf_sigmoid;
 /* stochastic.sigmoidCombine (matrix.hh:668-677) */

@@ -127,8 +127,8 @@ int oc_resolve(const pf_field_desc* d, oc_geom* g, char* err, int errlen) {
   if (d->anisotropy < 0 || d->anisotropy > 2)
     FAIL("stochastic.anisotropy must be \"none\", \"axiparallel\" or \"geometric\"");
   /* matrix.hh:515-579 */
-  if (d->periodization < 0 || d->periodization > 1) FAIL("embedding.periodization must be classical or merge");
-  if (d->periodization == PF_PERIODIZATION_MERGE) {
+  if (d->periodization < 0 || d->periodization > 2) FAIL("embedding.periodization must be classical, merge or fold");
+  if (d->periodization != PF_PERIODIZATION_CLASSICAL) {
     if (d->sigmoid < 0 || d->sigmoid > 1) FAIL("embedding.sigmoid must be \"smooth\" or \"smoothstep\"");
     if (d->sigmoid_combine < 0 || d->sigmoid_combine > 2) FAIL("sigmoidCombine must be tensor, radial or radialPlus");
   }
@@ -745,9 +745,10 @@ static double oc_sigmoid(int kind, double oneEdge, double zeroEdge, double x, un
   return output;
 }
 
-/* mergeRecursions default 99 (matrix.hh:693-717) */
+/* mergeRecursions / foldRecursions default 99 (matrix.hh:693-717, 803-827) */
 static unsigned int oc_merge_recursions(const pf_field_desc* d) {
-  if (d->merge_recursions != 99) return (unsigned int)d->merge_recursions;
+  const int r = d->periodization == PF_PERIODIZATION_FOLD ? d->fold_recursions : d->merge_recursions;
+  if (r != 99) return (unsigned int)r;
   switch (d->covariance) {
     case PF_COV_MATERN: return (unsigned int)floor(d->matern_nu * 2. + d->dim / 2.);
     case PF_COV_GAMMA_EXPONENTIAL: return (unsigned int)floor(d->exp_gamma + d->dim / 2.);
@@ -799,6 +800,44 @@ static double oc_merge_value(const pf_field_desc* d, const oc_geom* g, const dou
   return value + constValue * remainder;
 }
 
+/* adaptive Simpson quadrature of the fold sigmoid (in place of GSL's qng) */
+static double oc_fold_sig(const pf_field_desc* d, double beta, unsigned int rec, double x) {
+  return oc_sigmoid(d->sigmoid, 1., beta, x, rec);
+}
+static double oc_simpson(const pf_field_desc* d, double beta, unsigned int rec, double a, double b, double fa,
+                         double fm, double fb, double whole, int depth) {
+  const double m = 0.5 * (a + b), lm = 0.5 * (a + m), rm = 0.5 * (m + b);
+  const double flm = oc_fold_sig(d, beta, rec, lm), frm = oc_fold_sig(d, beta, rec, rm);
+  const double left = (m - a) / 6. * (fa + 4. * flm + fm), right = (b - m) / 6. * (fm + 4. * frm + fb);
+  if (depth <= 0 || fabs(left + right - whole) <= 1e-15 * 15.) return left + right + (left + right - whole) / 15.;
+  return oc_simpson(d, beta, rec, a, m, fa, flm, fm, left, depth - 1) +
+         oc_simpson(d, beta, rec, m, b, fm, frm, fb, right, depth - 1);
+}
+
+/* computeMatrixEntriesWithFold (matrix.hh:791-890) at classical coordinates coord */
+static double oc_fold_value(const pf_field_desc* d, const oc_geom* g, double* coord) {
+  const int dim = g->dim;
+  const double beta = d->fold_max_factor * 0.5 * g->factor / sqrt((double)dim);
+  const unsigned int rec = oc_merge_recursions(d);
+  double norm = 0.;
+  for (int i = 0; i < dim; i++) norm += (coord[i] * coord[i]) / (g->ext[i] * g->ext[i]);
+  norm = sqrt(norm / (double)dim);
+  if (norm > 1.) {
+    const double hi = norm < beta ? norm : beta;
+    double val = 0.;
+    if (hi > 1.) {
+      const double fa = oc_fold_sig(d, beta, rec, 1.), fb = oc_fold_sig(d, beta, rec, hi);
+      const double fm = oc_fold_sig(d, beta, rec, 0.5 * (1. + hi));
+      val = oc_simpson(d, beta, rec, 1., hi, fa, fm, fb, (hi - 1.) / 6. * (fa + 4. * fm + fb), 40);
+    }
+    val += 1.;
+    for (int i = 0; i < dim; i++) coord[i] *= val / norm;
+  }
+  double tc[3] = {0, 0, 0};
+  oc_geometry(d, coord, tc);
+  return oc_covariance(d, tc);
+}
+
 int oc_fill_matrix(const pf_field_desc* d, double* out, uint64_t count) {
   oc_geom g;
   int st = oc_resolve(d, &g, NULL, 0);
@@ -826,6 +865,10 @@ int oc_fill_matrix(const pf_field_desc* d, double* out, uint64_t count) {
       r /= cells[i];
       coord[i] = (double)ii * g.h[i];
       if (coord[i] > 0.5 * g.ext[i] * fac) coord[i] -= g.ext[i] * fac;
+    }
+    if (d->periodization == PF_PERIODIZATION_FOLD) {
+      out[idx] = oc_fold_value(d, &g, coord);
+      continue;
     }
     oc_geometry(d, coord, tc);
     out[idx] = oc_covariance(d, tc);

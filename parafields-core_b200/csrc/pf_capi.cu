@@ -149,14 +149,16 @@ static pf_status resolve(const pf_field_desc* d, Geom* g) {
   if (c == PF_COV_CUBIC && d->dim == 3) return fail(PF_ERR_CONFIG, "cubic covariance only applicable in 1D or 2D");
   if (d->anisotropy < 0 || d->anisotropy > 2)
     return fail(PF_ERR_CONFIG, "stochastic.anisotropy must be \"none\", \"axiparallel\" or \"geometric\"");
-  if (d->periodization < 0 || d->periodization > 1)
-    return fail(PF_ERR_CONFIG, "embedding.periodization must be \"classical\" or \"merge\" (fold and cofold are not built)");
-  if (d->periodization == PF_PERIODIZATION_MERGE) {
+  if (d->periodization < 0 || d->periodization > 2)
+    return fail(PF_ERR_CONFIG,
+                "embedding.periodization must be \"classical\", \"merge\" or \"fold\" (cofold is not built)");
+  if (d->periodization != PF_PERIODIZATION_CLASSICAL) {
     if (d->sigmoid < 0 || d->sigmoid > 1)
       return fail(PF_ERR_CONFIG, "embedding.sigmoid must be \"smooth\" or \"smoothstep\"");
     if (d->sigmoid_combine < 0 || d->sigmoid_combine > 2)
       return fail(PF_ERR_CONFIG, "sigmoidCombine must be tensor, radial or radialPlus");
-    if (d->merge_recursions == 99 && c != PF_COV_MATERN && c != PF_COV_GAMMA_EXPONENTIAL &&
+    const int rq = d->periodization == PF_PERIODIZATION_MERGE ? d->merge_recursions : d->fold_recursions;
+    if (rq == 99 && c != PF_COV_MATERN && c != PF_COV_GAMMA_EXPONENTIAL &&
         c != PF_COV_GENERALIZED_CAUCHY && c != PF_COV_EXPONENTIAL && c != PF_COV_MATERN32 &&
         c != PF_COV_MATERN52 && c != PF_COV_CAUCHY)
       return fail(PF_ERR_CONFIG, "magic recursions value 99 not implemented for choice of covariance");
@@ -720,6 +722,29 @@ static unsigned grid_for(uint64_t n) {
 // ---------------------------------------------------------------------------
 // spectrum: fillTransformedMatrix (matrix.hh:223-318)
 // ---------------------------------------------------------------------------
+// Gauss-Legendre nodes and weights on [-1, 1] (Newton iteration on P_n from the
+// asymptotic initial guesses), for the fold integrals
+static void gauss_legendre(int n, double* x, double* w) {
+  const double pi = 3.141592653589793238462643383279502884;
+  for (int i = 0; i < n; i++) {
+    double z = std::cos(pi * (i + 0.75) / (n + 0.5)), dp = 1.;
+    for (int it = 0; it < 100; it++) {
+      double p0 = 1., p1 = z;
+      for (int k = 2; k <= n; k++) {
+        const double p2 = ((2. * k - 1.) * z * p1 - (k - 1.) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = n * (z * p1 - p0) / (z * z - 1.);
+      const double dz = p1 / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    x[i] = z;
+    w[i] = 2. / ((1. - z * z) * dp * dp);
+  }
+}
+
 static CovParams cov_params(const pf_field_desc* d, const Geom& g) {
   CovParams c{};
   c.dim = g.dim;
@@ -782,8 +807,10 @@ static CovParams cov_params(const pf_field_desc* d, const Geom& g) {
   c.sstart = d->sigmoid_start;
   c.send = d->sigmoid_end < 0 ? (double)g.factor - 1. : d->sigmoid_end;
   for (int i = 0; i < 3; i++) c.ext[i] = g.ext[i];
-  int rec = d->merge_recursions;
-  if (rec == 99) {  // matrix.hh:693-717
+  int rec = d->periodization == PF_PERIODIZATION_FOLD ? d->fold_recursions : d->merge_recursions;
+  c.fold_beta = d->fold_max_factor * 0.5 * (double)g.factor / std::sqrt((double)g.dim);  // matrix.hh:839-842
+  gauss_legendre(kFoldNodes, c.gl_x, c.gl_w);
+  if (rec == 99) {  // matrix.hh:693-717, 803-827
     const double hd = (double)g.dim / 2.;
     switch (d->covariance) {
       case PF_COV_MATERN: rec = (int)std::floor(d->matern_nu * 2. + hd); break;
@@ -1398,6 +1425,8 @@ void pf_field_desc_init(pf_field_desc* d) {
   d->merge_recursions = 99;
   d->sigmoid_start = 1.0;
   d->sigmoid_end = -1.0;
+  d->fold_max_factor = 1.0;
+  d->fold_recursions = 99;
 }
 
 pf_status pf_plan_create(const pf_field_desc* desc, pf_plan** plan) {

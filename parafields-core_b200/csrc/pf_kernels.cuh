@@ -403,7 +403,11 @@ struct CovParams {
   int rec;          // sigmoid recursions
   double sstart, send, factor;
   double ext[3];
+  // fold periodization (matrix.hh:791-890): zero edge of the sigmoid and Gauss-Legendre rule
+  double fold_beta;
+  double gl_x[16], gl_w[16];
 };
+constexpr int kFoldNodes = 16;
 
 // Modified Bessel function of the second kind K_nu(x), nu >= 0, x > 0.
 // Temme's series (N. M. Temme, J. Comput. Phys. 19, 324-337, 1975) for x <= 2 and
@@ -642,10 +646,49 @@ __device__ __noinline__ double cov_merge(const CovParams& c, const int* jj) {
   return value + cst * remainder;
 }
 
-// covariance at torus cell (j0, j1, j2) with the classical mirroring (or the merge)
+// integral of the sigmoid (one edge 1, zero edge beta) from 1 to b > 1: zero beyond beta;
+// below it a polynomial (smoothstep, exact with 16 Gauss-Legendre nodes up to 15
+// recursions) or the smooth sigmoid (32 panels of 16 nodes)
+__device__ __noinline__ double fold_integral(const CovParams& c, double b) {
+  const double hi = b < c.fold_beta ? b : c.fold_beta;
+  if (hi <= 1.) return 0.;
+  const int panels = c.sig ? 32 : (c.rec <= 15 ? 1 : 8);
+  const double wdt = (hi - 1.) / panels;
+  double s = 0.;
+  for (int p = 0; p < panels; p++) {
+    const double a0 = 1. + p * wdt, mid = a0 + 0.5 * wdt;
+    double q = 0.;
+    for (int k = 0; k < kFoldNodes; k++) q += c.gl_w[k] * sigmoid_of(c, 1., c.fold_beta, mid + 0.5 * wdt * c.gl_x[k]);
+    s += 0.5 * wdt * q;
+  }
+  return s;
+}
+
+// computeMatrixEntriesWithFold (matrix.hh:791-890): classical coordinates, and beyond the
+// normalized radius 1 the radius r is replaced by 1 + integral_1^r sigmoid
+__device__ __noinline__ double cov_fold(const CovParams& c, const int* jj) {
+  double x[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
+  double norm = 0.;
+  for (int i = 0; i < c.dim; i++) {
+    double v = (double)(unsigned int)jj[i] * c.h[i];
+    if (v > c.half[i]) v -= c.wrap[i];
+    x[i] = v;
+    norm += (v * v) / (c.ext[i] * c.ext[i]);
+  }
+  norm = sqrt(norm / (double)c.dim);
+  if (norm > 1.) {
+    const double val = fold_integral(c, norm) + 1.;
+    for (int i = 0; i < c.dim; i++) x[i] *= val / norm;
+  }
+  geo_apply(c, x, xt);
+  return cov_eval(c, xt);
+}
+
+// covariance at torus cell (j0, j1, j2) with the classical mirroring (or merge / fold)
 __device__ __forceinline__ double cov_at(const CovParams& c, int j0, int j1, int j2) {
   const int jj[3] = {j0, j1, j2};
   if (c.per == 1) return cov_merge(c, jj);
+  if (c.per == 2) return cov_fold(c, jj);
   double x[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
   for (int i = 0; i < c.dim; i++) {
     double v = (double)(unsigned int)jj[i] * c.h[i];

@@ -96,8 +96,10 @@ pf_field_desc descFromConfig(const ParameterTree& config) {
   d.threshold = config.get<double>("embedding.threshold", 1e-14);
   if (config.hasKey("fftw.transposed")) d.transposed = config.get<bool>("fftw.transposed") ? 1 : 0;
   const std::string per = config.get<std::string>("embedding.periodization", std::string("classical"));
-  if (per == "merge") {
-    d.periodization = PF_PERIODIZATION_MERGE;
+  if (per == "merge" || per == "fold") {
+    d.periodization = per == "merge" ? PF_PERIODIZATION_MERGE : PF_PERIODIZATION_FOLD;
+    d.fold_max_factor = config.get<double>("embedding.foldMaxFactor", 1.);
+    d.fold_recursions = (int32_t)config.get<unsigned>("embedding.foldRecursions", 99u);
     const std::string sig = config.get<std::string>("embedding.sigmoid", std::string("smoothstep"));
     if (sig == "smooth")
       d.sigmoid = PF_SIGMOID_SMOOTH;

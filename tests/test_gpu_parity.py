@@ -58,6 +58,12 @@ CONFIGS = {
                                    corr_length=(0.2, 0.05, -0.05, 0.15), anisotropy="geometric",
                                    embedding_factor=4, periodization="merge", sigmoid_combine="radial",
                                    sigmoid_start=1.0, sigmoid_end=3.0, approximate=True),
+    # fold periodization (matrix.hh:791-890)
+    "2d-fold-smoothstep-f3": dict(dim=2, cells=(48, 40), covariance="exponential", corr_length=0.3,
+                                  embedding_factor=3, periodization="fold", approximate=True),
+    "3d-fold-smooth": dict(dim=3, cells=(16, 16, 12), covariance="matern32", corr_length=(0.2, 0.1, 0.1),
+                           anisotropy="axiparallel", periodization="fold", sigmoid="smooth",
+                           fold_max_factor=2.0, approximate=True),
     # tori whose lengths have prime factors above 13: Bluestein transforms
     "2d-exp-prime": dict(dim=2, cells=(131, 97), covariance="exponential", corr_length=0.1),
     "3d-sph-prime": dict(dim=3, cells=(17, 19, 23), covariance="spherical", corr_length=0.2),

@@ -239,3 +239,24 @@ def test_merge_periodization_smooths_the_embedding(oracle):
     inside = (np.arange(g.T[1] // 2 + 1)[:, None] < g.n[1]) & (np.arange(g.T[0] // 2 + 1)[None, :] < g.n[0])
     assert np.abs(a[inside] - b[inside]).max() < 1e-12
     assert np.abs(a[~inside] - b[~inside]).max() > 1e-6
+
+
+def test_fold_periodization_keeps_domain_and_stretches_beyond(oracle):
+    """embedding.periodization = fold (matrix.hh:791-890): within normalized radius 1 the
+    covariance is the classical one; beyond it the radius r becomes 1 + int_1^r sigmoid, so
+    the folded covariance at a cell equals the classical covariance at a shorter radius
+    (never larger distance) and lies between the classical value and the value at radius 1."""
+    import pfb200
+    for sig in ("smoothstep", "smooth"):
+        kw = dict(dim=2, cells=(16, 12), covariance="exponential", corr_length=0.5, embedding_factor=3)
+        base = pfb200.make_desc(**kw)
+        fold = pfb200.make_desc(**kw, periodization="fold", sigmoid=sig, fold_max_factor=1.0)
+        g = oracle.resolve(base)
+        a = oracle.fill_matrix(base).reshape(g.T[1] // 2 + 1, g.T[0] // 2 + 1)
+        b = oracle.fill_matrix(fold).reshape(g.T[1] // 2 + 1, g.T[0] // 2 + 1)
+        y, x = np.meshgrid(np.arange(g.T[1] // 2 + 1) * g.h[1], np.arange(g.T[0] // 2 + 1) * g.h[0], indexing="ij")
+        r = np.sqrt((x ** 2 + y ** 2) / 2.0)
+        inside = r <= 1.0
+        assert np.abs(a[inside] - b[inside]).max() < 1e-14
+        assert (b[~inside] >= a[~inside] - 1e-15).all()
+        assert np.abs(a[~inside] - b[~inside]).max() > 1e-3
