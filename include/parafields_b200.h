@@ -157,15 +157,18 @@ typedef struct pf_field_desc {
   double sigmoid_end;        /* embedding.sigmoidEnd (negative: default factor - 1) */
   double fold_max_factor;    /* embedding.foldMaxFactor (default 1) */
   int32_t fold_recursions;   /* embedding.foldRecursions (99: the covariance's default) */
-  int32_t pad_;
+  int32_t cofold_recursions; /* embedding.cofoldRecursions (default 1) */
+  double cofold_max_factor;  /* embedding.cofoldMaxFactor (default 5) */
 } pf_field_desc;
 
 /* embedding.periodization: classical mirroring, sigmoid merging of the 2^d mirrored copies,
- * or folding of the distances beyond the domain (cofold is not built) */
+ * folding of the distances beyond the domain, or cofolding of the covariance values beyond
+ * the domain (cofold: DCT matrix backend, i.e. anisotropy none / axiparallel) */
 typedef enum pf_periodization {
   PF_PERIODIZATION_CLASSICAL = 0,
   PF_PERIODIZATION_MERGE = 1,
-  PF_PERIODIZATION_FOLD = 2
+  PF_PERIODIZATION_FOLD = 2,
+  PF_PERIODIZATION_COFOLD = 3
 } pf_periodization;
 /* embedding.sigmoid (covariance.hh:147-287) */
 typedef enum pf_sigmoid { PF_SIGMOID_SMOOTHSTEP = 0, PF_SIGMOID_SMOOTH = 1 } pf_sigmoid;

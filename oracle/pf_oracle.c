@@ -127,10 +127,14 @@ int oc_resolve(const pf_field_desc* d, oc_geom* g, char* err, int errlen) {
   if (d->anisotropy < 0 || d->anisotropy > 2)
     FAIL("stochastic.anisotropy must be \"none\", \"axiparallel\" or \"geometric\"");
   /* matrix.hh:515-579 */
-  if (d->periodization < 0 || d->periodization > 2) FAIL("embedding.periodization must be classical, merge or fold");
+  if (d->periodization < 0 || d->periodization > 3)
+    FAIL("stochastic.periodization must be \"classical\", \"merge\", \"fold\", or \"cofold\"");
   if (d->periodization != PF_PERIODIZATION_CLASSICAL) {
     if (d->sigmoid < 0 || d->sigmoid > 1) FAIL("embedding.sigmoid must be \"smooth\" or \"smoothstep\"");
-    if (d->sigmoid_combine < 0 || d->sigmoid_combine > 2) FAIL("sigmoidCombine must be tensor, radial or radialPlus");
+    if (d->periodization != PF_PERIODIZATION_COFOLD && (d->sigmoid_combine < 0 || d->sigmoid_combine > 2))
+      FAIL("sigmoidCombine must be tensor, radial or radialPlus");
+    if (d->periodization == PF_PERIODIZATION_COFOLD && d->cofold_recursions < 0)
+      FAIL("embedding.cofoldRecursions must be non-negative");
   }
 #undef FAIL
   return PF_OK;
@@ -838,6 +842,79 @@ static double oc_fold_value(const pf_field_desc* d, const oc_geom* g, double* co
   return oc_covariance(d, tc);
 }
 
+/* integrand of the cofold integral: sigmoid(0, beta - alpha, beta - t) (matrix.hh:956-962) */
+static double oc_cofold_sig(const pf_field_desc* d, double alpha, double beta, double t) {
+  return oc_sigmoid(d->sigmoid, 0., beta - alpha, beta - t, (unsigned int)d->cofold_recursions);
+}
+static double oc_cofold_simpson(const pf_field_desc* d, double alpha, double beta, double a, double b, double fa,
+                                double fm, double fb, double whole, int depth) {
+  const double m = 0.5 * (a + b), lm = 0.5 * (a + m), rm = 0.5 * (m + b);
+  const double flm = oc_cofold_sig(d, alpha, beta, lm), frm = oc_cofold_sig(d, alpha, beta, rm);
+  const double left = (m - a) / 6. * (fa + 4. * flm + fm), right = (b - m) / 6. * (fm + 4. * frm + fb);
+  if (depth <= 0 || fabs(left + right - whole) <= 15. * 1e-15 * fabs(b - a))
+    return left + right + (left + right - whole) / 15.;
+  return oc_cofold_simpson(d, alpha, beta, a, m, fa, flm, fm, left, depth - 1) +
+         oc_cofold_simpson(d, alpha, beta, m, b, fm, frm, fb, right, depth - 1);
+}
+/* signed integral over [a, b] by adaptive Simpson quadrature (in place of GSL's qng) */
+static double oc_cofold_integral(const pf_field_desc* d, double alpha, double beta, double a, double b) {
+  if (a == b) return 0.;
+  const double fa = oc_cofold_sig(d, alpha, beta, a), fb = oc_cofold_sig(d, alpha, beta, b);
+  const double fm = oc_cofold_sig(d, alpha, beta, 0.5 * (a + b));
+  return oc_cofold_simpson(d, alpha, beta, a, b, fa, fm, fb, (b - a) / 6. * (fa + 4. * fm + fb), 30);
+}
+
+/* classical coordinates and the cofold norm max_i |coord_i| / ext_i of matrix cell idx
+ * (matrix.hh:917-931) */
+static double oc_cofold_coord(const oc_geom* g, const int* cells, uint64_t idx, double* coord) {
+  const double fac = (double)g->factor;
+  uint64_t r = idx;
+  double norm = 0.;
+  for (int i = 0; i < g->dim; i++) {
+    const unsigned int ii = (unsigned int)(r % (uint64_t)cells[i]);
+    r /= (uint64_t)cells[i];
+    coord[i] = (double)ii * g->h[i];
+    if (coord[i] > 0.5 * g->ext[i] * fac) coord[i] -= g->ext[i] * fac;
+  }
+  for (int i = 0; i < g->dim; i++)
+    if (fabs(coord[i]) / g->ext[i] > norm) norm = fabs(coord[i]) / g->ext[i];
+  return norm;
+}
+
+/* modifyMatrixEntriesWithCofold (matrix.hh:905-1013) on the classically filled matrix */
+static void oc_cofold_modify(const pf_field_desc* d, const oc_geom* g, const int* cells, double* m,
+                             uint64_t total) {
+  const double fac = (double)g->factor;
+  double minConstrained = 1.7976931348623157e308, maxBorder = -1.7976931348623157e308;
+  for (uint64_t idx = 0; idx < total; idx++) {
+    double coord[3] = {0, 0, 0};
+    const double norm = oc_cofold_coord(g, cells, idx, coord);
+    const double val = m[idx];
+    if (norm <= 1.) {
+      if (val < minConstrained) minConstrained = val;
+    } else {
+      for (int i = 0; i < g->dim; i++)
+        if (val > maxBorder && 0.5 * g->ext[i] * fac - fabs(coord[i]) < g->ext[i] / (double)g->T[i])
+          maxBorder = val;
+    }
+  }
+  const double alpha = maxBorder;
+  const double mf = d->cofold_max_factor * maxBorder;
+  const double beta = minConstrained < mf ? minConstrained : mf;
+  const double offset = beta - oc_cofold_integral(d, alpha, beta, alpha, beta);
+#pragma omp parallel for schedule(static)
+  for (long long idx = 0; idx < (long long)total; idx++) {
+    double coord[3] = {0, 0, 0};
+    if (oc_cofold_coord(g, cells, (uint64_t)idx, coord) > 1.) {
+      const double x = m[idx];
+      if (x < alpha)
+        m[idx] = offset;
+      else if (x < beta)
+        m[idx] = oc_cofold_integral(d, alpha, beta, alpha, x) + offset;
+    }
+  }
+}
+
 int oc_fill_matrix(const pf_field_desc* d, double* out, uint64_t count) {
   oc_geom g;
   int st = oc_resolve(d, &g, NULL, 0);
@@ -873,6 +950,7 @@ int oc_fill_matrix(const pf_field_desc* d, double* out, uint64_t count) {
     oc_geometry(d, coord, tc);
     out[idx] = oc_covariance(d, tc);
   }
+  if (d->periodization == PF_PERIODIZATION_COFOLD) oc_cofold_modify(d, &g, cells, out, total);
   return PF_OK;
 }
 

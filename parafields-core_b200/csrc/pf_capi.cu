@@ -149,12 +149,15 @@ static pf_status resolve(const pf_field_desc* d, Geom* g) {
   if (c == PF_COV_CUBIC && d->dim == 3) return fail(PF_ERR_CONFIG, "cubic covariance only applicable in 1D or 2D");
   if (d->anisotropy < 0 || d->anisotropy > 2)
     return fail(PF_ERR_CONFIG, "stochastic.anisotropy must be \"none\", \"axiparallel\" or \"geometric\"");
-  if (d->periodization < 0 || d->periodization > 2)
+  if (d->periodization < 0 || d->periodization > 3)
     return fail(PF_ERR_CONFIG,
-                "embedding.periodization must be \"classical\", \"merge\" or \"fold\" (cofold is not built)");
-  if (d->periodization != PF_PERIODIZATION_CLASSICAL) {
-    if (d->sigmoid < 0 || d->sigmoid > 1)
-      return fail(PF_ERR_CONFIG, "embedding.sigmoid must be \"smooth\" or \"smoothstep\"");
+                "stochastic.periodization must be \"classical\", \"merge\", \"fold\", or \"cofold\"");
+  if (d->periodization != PF_PERIODIZATION_CLASSICAL &&
+      (d->sigmoid < 0 || d->sigmoid > 1))
+    return fail(PF_ERR_CONFIG, "embedding.sigmoid must be \"smooth\" or \"smoothstep\"");
+  if (d->periodization == PF_PERIODIZATION_COFOLD && d->cofold_recursions < 0)
+    return fail(PF_ERR_CONFIG, "embedding.cofoldRecursions must be non-negative");
+  if (d->periodization == PF_PERIODIZATION_MERGE || d->periodization == PF_PERIODIZATION_FOLD) {
     if (d->sigmoid_combine < 0 || d->sigmoid_combine > 2)
       return fail(PF_ERR_CONFIG, "sigmoidCombine must be tensor, radial or radialPlus");
     const int rq = d->periodization == PF_PERIODIZATION_MERGE ? d->merge_recursions : d->fold_recursions;
@@ -205,6 +208,7 @@ struct pf_plan {
   float* lam32 = nullptr;
   void* fac[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
   ScanOut* scan = nullptr;
+  double* cof = nullptr;  // cofold: 2 keys, then {active, alpha, beta, offset}
   // workspaces
   void* ws[3] = {nullptr, nullptr, nullptr};
   size_t ws_bytes[3] = {0, 0, 0};
@@ -808,6 +812,7 @@ static CovParams cov_params(const pf_field_desc* d, const Geom& g) {
   c.send = d->sigmoid_end < 0 ? (double)g.factor - 1. : d->sigmoid_end;
   for (int i = 0; i < 3; i++) c.ext[i] = g.ext[i];
   int rec = d->periodization == PF_PERIODIZATION_FOLD ? d->fold_recursions : d->merge_recursions;
+  if (d->periodization == PF_PERIODIZATION_COFOLD) rec = d->cofold_recursions;  // no magic value
   c.fold_beta = d->fold_max_factor * 0.5 * (double)g.factor / std::sqrt((double)g.dim);  // matrix.hh:839-842
   gauss_legendre(kFoldNodes, c.gl_x, c.gl_w);
   if (rec == 99) {  // matrix.hh:693-717, 803-827
@@ -853,6 +858,24 @@ static pf_status build_spectrum(pf_plan* P) {
   CovRowLoad cl;
   cl.c = cov_params(d, g);
   const int dim = g.dim;
+  if (d->periodization == PF_PERIODIZATION_COFOLD) {
+    // statistics of the classical values over the matrix cells, then alpha, beta and the
+    // offset on the device; the spectrum passes below apply the value map
+    if (!P->cof) TRY(dalloc(P, (void**)&P->cof, 6 * sizeof(double)));
+    static const unsigned long long init[2] = {~0ull, 0ull};
+    CK(cudaMemcpyAsync(P->cof, init, sizeof(init), cudaMemcpyHostToDevice, P->stream));
+    int C[3] = {1, 1, 1};
+    for (int i = 0; i < dim; i++) C[i] = g.mb == PF_MATRIX_DCT ? g.T[i] / 2 + 1 : g.T[i];
+    CovParams sc = cl.c;
+    sc.per = 0;
+    unsigned long long* keys = (unsigned long long*)P->cof;
+    ProfRec rec;
+    TRY(prof_begin(P, "spec_cofold_stats", 0.0, &rec));
+    k_cofold_stats<<<grid_for((uint64_t)C[0] * C[1] * C[2]), kThreads, 0, P->stream>>>(sc, C[0], C[1], C[2], keys);
+    k_cofold_finish<<<1, 32, 0, P->stream>>>(sc, d->cofold_max_factor, keys, P->cof + 2);
+    TRY(prof_end(P, &rec));
+    cl.c.cof = P->cof + 2;
+  }
   void *A = nullptr, *Bw = nullptr;
   double2* spec = nullptr;
   const uint64_t full = g.mb == PF_MATRIX_DFT ? g.N : g.Nc;
@@ -1427,6 +1450,8 @@ void pf_field_desc_init(pf_field_desc* d) {
   d->sigmoid_end = -1.0;
   d->fold_max_factor = 1.0;
   d->fold_recursions = 99;
+  d->cofold_max_factor = 5.0;
+  d->cofold_recursions = 1;
 }
 
 pf_status pf_plan_create(const pf_field_desc* desc, pf_plan** plan) {
@@ -1458,7 +1483,7 @@ void pf_plan_destroy(pf_plan* P) {
   if (!P) return;
   cudaStreamSynchronize(P->stream);
   void** bufs[] = {(void**)&P->lam64, (void**)&P->sq64, (void**)&P->sq32, (void**)&P->lam32, (void**)&P->scan,
-                   &P->ws[0], &P->ws[1], &P->ws[2], (void**)&P->noise_dev, &P->io_dev, &P->io2_dev, &P->spare};
+                   (void**)&P->cof, &P->ws[0], &P->ws[1], &P->ws[2], (void**)&P->noise_dev, &P->io_dev, &P->io2_dev, &P->spare};
   for (void** b : bufs)
     if (*b) cudaFree(*b), *b = nullptr;
   for (int a = 0; a < 2; a++)

@@ -406,6 +406,9 @@ struct CovParams {
   // fold periodization (matrix.hh:791-890): zero edge of the sigmoid and Gauss-Legendre rule
   double fold_beta;
   double gl_x[16], gl_w[16];
+  // cofold periodization (matrix.hh:905-1013): {active, alpha, beta, offset} on the device,
+  // written by k_cofold_finish before the spectrum passes read it
+  const double* cof;
 };
 constexpr int kFoldNodes = 16;
 
@@ -684,17 +687,45 @@ __device__ __noinline__ double cov_fold(const CovParams& c, const int* jj) {
   return cov_eval(c, xt);
 }
 
-// covariance at torus cell (j0, j1, j2) with the classical mirroring (or merge / fold)
-__device__ __forceinline__ double cov_at(const CovParams& c, int j0, int j1, int j2) {
-  const int jj[3] = {j0, j1, j2};
-  if (c.per == 1) return cov_merge(c, jj);
-  if (c.per == 2) return cov_fold(c, jj);
-  double x[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
+// signed integral over [a, b] of the cofold integrand sigmoid(0, beta - alpha, beta - t):
+// the smoothstep is a polynomial (exact with 16 Gauss-Legendre nodes up to 15 recursions),
+// the smooth sigmoid takes 32 panels of 16 nodes
+__device__ __noinline__ double cofold_integral(const CovParams& c, double alpha, double beta, double a, double b) {
+  const int panels = c.sig ? 32 : (c.rec <= 15 ? 1 : 8);
+  const double wdt = (b - a) / panels;
+  double s = 0.;
+  for (int p = 0; p < panels; p++) {
+    const double mid = a + (p + 0.5) * wdt;
+    double q = 0.;
+    for (int k = 0; k < kFoldNodes; k++)
+      q += c.gl_w[k] * sigmoid_of(c, 0., beta - alpha, beta - (mid + 0.5 * wdt * c.gl_x[k]));
+    s += 0.5 * wdt * q;
+  }
+  return s;
+}
+
+// classical coordinates of torus cell jj (computeMatrixEntriesWithMirroring, matrix.hh:615-638)
+__device__ __forceinline__ void classical_coord(const CovParams& c, const int* jj, double* x) {
   for (int i = 0; i < c.dim; i++) {
     double v = (double)(unsigned int)jj[i] * c.h[i];
     if (v > c.half[i]) v -= c.wrap[i];
     x[i] = v;
   }
+}
+
+// cofold norm: largest |coordinate| / extension over the axes (matrix.hh:928-931)
+__device__ __forceinline__ double cofold_norm(const CovParams& c, const double* x) {
+  double norm = 0.;
+  for (int i = 0; i < c.dim; i++) {
+    const double r = __ddiv_rn(fabs(x[i]), c.ext[i]);
+    if (r > norm) norm = r;
+  }
+  return norm;
+}
+
+// covariance of the classically wrapped coordinates x
+__device__ __forceinline__ double cov_classical(const CovParams& c, const double* x) {
+  double xt[3] = {0, 0, 0};
   if (c.aniso == 0) {
     for (int i = 0; i < c.dim; i++) xt[i] = c.geo[0] * x[i];
   } else if (c.aniso == 1) {
@@ -707,6 +738,30 @@ __device__ __forceinline__ double cov_at(const CovParams& c, int j0, int j1, int
     }
   }
   return cov_eval(c, xt);
+}
+
+// modifyMatrixEntriesWithCofold (matrix.hh:983-1001): beyond norm 1 the values below alpha
+// become the offset, those in [alpha, beta) the offset plus the integral of the sigmoid
+__device__ __noinline__ double cov_cofold(const CovParams& c, const int* jj) {
+  double x[3] = {0, 0, 0};
+  classical_coord(c, jj, x);
+  const double v = cov_classical(c, x);
+  if (c.cof[0] == 0. || !(cofold_norm(c, x) > 1.)) return v;
+  const double alpha = c.cof[1], beta = c.cof[2], offset = c.cof[3];
+  if (v < alpha) return offset;
+  if (v < beta) return cofold_integral(c, alpha, beta, alpha, v) + offset;
+  return v;
+}
+
+// covariance at torus cell (j0, j1, j2) with the classical mirroring (or merge / fold / cofold)
+__device__ __forceinline__ double cov_at(const CovParams& c, int j0, int j1, int j2) {
+  const int jj[3] = {j0, j1, j2};
+  if (c.per == 1) return cov_merge(c, jj);
+  if (c.per == 2) return cov_fold(c, jj);
+  if (c.per == 3) return cov_cofold(c, jj);
+  double x[3] = {0, 0, 0};
+  classical_coord(c, jj, x);
+  return cov_classical(c, x);
 }
 
 // row p of the torus (dims 1..d-1 flattened), element j along dim 0
@@ -1094,6 +1149,68 @@ struct ScanOut {
 __device__ __forceinline__ unsigned long long dkey(double v) {
   unsigned long long b = (unsigned long long)__double_as_longlong(v);
   return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+// key of an ordered key back to the double (inverse of dkey)
+__device__ __forceinline__ double dkey_value(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
+// Statistics of modifyMatrixEntriesWithCofold (matrix.hh:913-945) over the matrix cells
+// C0 x C1 x C2 (the T/2+1 cells per axis of the DCT matrix, the torus otherwise):
+// keys[0] = min key of the classical values with norm <= 1 (the constrained cells),
+// keys[1] = max key of those with norm > 1 within ext/T of half the torus on some axis.
+__global__ void __launch_bounds__(kThreads) k_cofold_stats(CovParams c, int C0, int C1, int C2,
+                                                           unsigned long long* keys) {
+  unsigned long long mn = ~0ull, mx = 0ull;
+  const uint64_t n = (uint64_t)C0 * C1 * C2;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t r = i / (uint64_t)C0;
+    const int jj[3] = {(int)(i % (uint64_t)C0), (int)(r % (uint64_t)C1), (int)(r / (uint64_t)C1)};
+    double x[3] = {0, 0, 0};
+    classical_coord(c, jj, x);
+    const double v = cov_classical(c, x);
+    if (cofold_norm(c, x) <= 1.) {
+      const unsigned long long k = dkey(v);
+      mn = k < mn ? k : mn;
+    } else {
+      bool border = false;
+      for (int a = 0; a < c.dim; a++)
+        if (c.half[a] - fabs(x[a]) < __ddiv_rn(c.ext[a], (double)(unsigned int)c.T[a])) border = true;
+      if (border) {
+        const unsigned long long k = dkey(v);
+        mx = k > mx ? k : mx;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long a = __shfl_xor_sync(0xffffffffu, mn, o), b = __shfl_xor_sync(0xffffffffu, mx, o);
+    mn = a < mn ? a : mn;
+    mx = b > mx ? b : mx;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (mn != ~0ull) atomicMin(&keys[0], mn);
+    if (mx != 0ull) atomicMax(&keys[1], mx);
+  }
+}
+
+// alpha = max border value, beta = min(max_factor * alpha, min constrained value),
+// offset = beta - integral_alpha^beta sigmoid (matrix.hh:947-972); cof = {active, alpha,
+// beta, offset}; inactive (identity) when either set of cells is empty
+__global__ void k_cofold_finish(CovParams c, double max_factor, const unsigned long long* keys, double* cof) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (keys[0] == ~0ull || keys[1] == 0ull) {
+    cof[0] = 0.;
+    return;
+  }
+  const double minc = dkey_value(keys[0]), alpha = dkey_value(keys[1]);
+  const double mf = max_factor * alpha;
+  const double beta = minc < mf ? minc : mf;
+  cof[0] = 1.;
+  cof[1] = alpha;
+  cof[2] = beta;
+  cof[3] = beta - cofold_integral(c, alpha, beta, alpha, beta);
 }
 
 struct ScanArgs {

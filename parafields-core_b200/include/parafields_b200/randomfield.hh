@@ -96,10 +96,13 @@ pf_field_desc descFromConfig(const ParameterTree& config) {
   d.threshold = config.get<double>("embedding.threshold", 1e-14);
   if (config.hasKey("fftw.transposed")) d.transposed = config.get<bool>("fftw.transposed") ? 1 : 0;
   const std::string per = config.get<std::string>("embedding.periodization", std::string("classical"));
-  if (per == "merge" || per == "fold") {
-    d.periodization = per == "merge" ? PF_PERIODIZATION_MERGE : PF_PERIODIZATION_FOLD;
+  if (per == "merge" || per == "fold" || per == "cofold") {
+    d.periodization = per == "merge" ? PF_PERIODIZATION_MERGE
+                                     : (per == "fold" ? PF_PERIODIZATION_FOLD : PF_PERIODIZATION_COFOLD);
     d.fold_max_factor = config.get<double>("embedding.foldMaxFactor", 1.);
     d.fold_recursions = (int32_t)config.get<unsigned>("embedding.foldRecursions", 99u);
+    d.cofold_max_factor = config.get<double>("embedding.cofoldMaxFactor", 5.);
+    d.cofold_recursions = (int32_t)config.get<double>("embedding.cofoldRecursions", 1.);
     const std::string sig = config.get<std::string>("embedding.sigmoid", std::string("smoothstep"));
     if (sig == "smooth")
       d.sigmoid = PF_SIGMOID_SMOOTH;
@@ -120,7 +123,8 @@ pf_field_desc descFromConfig(const ParameterTree& config) {
     d.sigmoid_end = config.get<double>("embedding.sigmoidEnd", (double)d.embedding_factor - 1.);
     d.merge_recursions = (int32_t)config.get<unsigned>("embedding.mergeRecursions", 99u);
   } else if (per != "classical") {
-    throw std::runtime_error{"embedding.periodization \"" + per + "\" is not available on the B200 path"};
+    throw std::runtime_error{
+        "stochastic.periodization must be \"classical\", \"merge\", \"fold\", or \"cofold\""};
   }
   const std::string optim = config.get<std::string>("embedding.optim", std::string("none"));
   if (optim != "none") throw std::runtime_error{"optimization requires dune-nonlinopt"};

@@ -30,7 +30,7 @@ COVARIANCES = {
 }
 ANISOTROPIES = {"none": 0, "axiparallel": 1, "geometric": 2}
 TRANSFORMS = {"none": 0, "logNormal": 1, "foldedNormal": 2, "sign": 3, "boxCox": 4}
-PERIODIZATIONS = {"classical": 0, "merge": 1, "fold": 2}
+PERIODIZATIONS = {"classical": 0, "merge": 1, "fold": 2, "cofold": 3}
 SIGMOIDS = {"smoothstep": 0, "smooth": 1}
 COMBINES = {"radialPlus": 0, "radial": 1, "tensor": 2}
 MATRIX_DCT, MATRIX_R2C, MATRIX_DFT = 0, 1, 2
@@ -54,7 +54,8 @@ class FieldDesc(C.Structure):
         ("transform", C.c_int32), ("boxcox_lambda", C.c_double),
         ("periodization", C.c_int32), ("sigmoid", C.c_int32), ("sigmoid_combine", C.c_int32),
         ("merge_recursions", C.c_int32), ("sigmoid_start", C.c_double), ("sigmoid_end", C.c_double),
-        ("fold_max_factor", C.c_double), ("fold_recursions", C.c_int32), ("pad_", C.c_int32),
+        ("fold_max_factor", C.c_double), ("fold_recursions", C.c_int32), ("cofold_recursions", C.c_int32),
+        ("cofold_max_factor", C.c_double),
     ]
 
 
@@ -98,7 +99,8 @@ def make_desc(dim=2, cells=(16, 16), extensions=None, covariance="exponential", 
               cg_iterations=100, transform="none", boxcox_lambda=0.0, matern_nu=0.5,
               exp_gamma=1.0, cauchy_alpha=1.0, cauchy_beta=1.0, periodization="classical",
               sigmoid="smoothstep", sigmoid_combine="radialPlus", merge_recursions=99,
-              sigmoid_start=1.0, sigmoid_end=-1.0, fold_max_factor=1.0, fold_recursions=99) -> FieldDesc:
+              sigmoid_start=1.0, sigmoid_end=-1.0, fold_max_factor=1.0, fold_recursions=99,
+              cofold_max_factor=5.0, cofold_recursions=1) -> FieldDesc:
     """Builds a descriptor from values named after the reference's config keys."""
     d = FieldDesc()
     d.dim = dim
@@ -140,6 +142,7 @@ def make_desc(dim=2, cells=(16, 16), extensions=None, covariance="exponential", 
     d.merge_recursions = merge_recursions
     d.sigmoid_start, d.sigmoid_end = sigmoid_start, sigmoid_end
     d.fold_max_factor, d.fold_recursions = fold_max_factor, fold_recursions
+    d.cofold_max_factor, d.cofold_recursions = cofold_max_factor, cofold_recursions
     return d
 
 

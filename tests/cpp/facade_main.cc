@@ -95,6 +95,9 @@ int main(int argc, char** argv) {
                   d.embedding_factor, d.periodic, d.covariance, d.variance, d.anisotropy, d.corr_length[0],
                   d.corr_length[1], d.corr_length[2], d.corr_length[3], d.approximate, d.threshold, d.transposed,
                   d.precision, d.eigen_check, d.cg_iterations, d.transform, d.boxcox_lambda, d.exp_gamma);
+      std::printf("per=%d sig=%d comb=%d mrec=%d sstart=%g send=%g fmf=%g frec=%d cmf=%g crec=%d\n", d.periodization,
+                  d.sigmoid, d.sigmoid_combine, d.merge_recursions, d.sigmoid_start, d.sigmoid_end, d.fold_max_factor,
+                  d.fold_recursions, d.cofold_max_factor, d.cofold_recursions);
       return 0;
     }
     const unsigned seed = (unsigned)std::stoul(argv[3]);

@@ -57,6 +57,22 @@ boxCoxLambda = 0.25
     assert "approx=1 thr=1e-12 transposed=-1 prec=0 eig=0 cg=50 transform=4 boxcox=0.25 gamma=1.2" in out
 
 
+@pytest.mark.parametrize("per,extra,want", [
+    ("merge", "sigmoid = smooth\nsigmoidStart = 0.5\nmergeRecursions = 3\n[stochastic]\nsigmoidCombine = tensor\n",
+     "per=1 sig=1 comb=2 mrec=3 sstart=0.5 send=2"),
+    ("fold", "foldMaxFactor = 2\nfoldRecursions = 4\n", "per=2 sig=0 comb=0 mrec=99 sstart=1 send=2 fmf=2 frec=4"),
+    ("cofold", "cofoldMaxFactor = 3\ncofoldRecursions = 2\n", "per=3 sig=0 comb=0 mrec=99 sstart=1 send=2 fmf=1 "
+     "frec=99 cmf=3 crec=2"),
+])
+def test_periodization_keys(facade_exe, tmp_path, per, extra, want):
+    """embedding.periodization and its sigmoid / merge / fold / cofold keys (matrix.hh:515-579,
+    652-1013) reach the descriptor."""
+    ini = write_ini(tmp_path, "[grid]\ncells = 16 16\nextensions = 1 1\n[stochastic]\nvariance = 1\ncovariance = exponential\n"
+                    "corrLength = 0.1\n[embedding]\nfactor = 3\nperiodization = " + per + "\n" + extra)
+    out = subprocess.run([facade_exe, "config", ini], capture_output=True, text=True).stdout
+    assert want in out, out
+
+
 @pytest.mark.parametrize("text,msg", [
     ("grid.cells = 8 8\ngrid.extensions = 1 1\nstochastic.variance = 1\nstochastic.covariance = foo\n"
      "stochastic.corrLength = 0.1\n", "covariance structure foo not known"),
@@ -64,6 +80,11 @@ boxCoxLambda = 0.25
      "stochastic.corrLength = 0.1\nstochastic.anisotropy = weird\n", "stochastic.anisotropy must be"),
     ("grid.cells = 8 8\ngrid.extensions = 1 1\nstochastic.variance = 1\nstochastic.covariance = exponential\n"
      "stochastic.corrLength = 0.1\nrandomField.transform = cube\n", "transform type not known"),
+    ("grid.cells = 8 8\ngrid.extensions = 1 1\nstochastic.variance = 1\nstochastic.covariance = exponential\n"
+     "stochastic.corrLength = 0.1\nembedding.periodization = twist\n", "stochastic.periodization must be"),
+    ("grid.cells = 8 8\ngrid.extensions = 1 1\nstochastic.variance = 1\nstochastic.covariance = exponential\n"
+     "stochastic.corrLength = 0.1\nembedding.periodization = cofold\nembedding.sigmoid = step\n",
+     "embedding.sigmoid must be"),
 ])
 def test_config_errors(facade_exe, tmp_path, text, msg):
     out = subprocess.run([facade_exe, "config", write_ini(tmp_path, text)], capture_output=True, text=True).stdout

@@ -64,6 +64,15 @@ CONFIGS = {
     "3d-fold-smooth": dict(dim=3, cells=(16, 16, 12), covariance="matern32", corr_length=(0.2, 0.1, 0.1),
                            anisotropy="axiparallel", periodization="fold", sigmoid="smooth",
                            fold_max_factor=2.0, approximate=True),
+    # cofold periodization (matrix.hh:905-1013): DCT matrix (iso / axiparallel) and R2C (geometric)
+    "2d-cofold-smoothstep-f3": dict(dim=2, cells=(48, 40), covariance="exponential", corr_length=0.3,
+                                    embedding_factor=3, periodization="cofold", approximate=True),
+    "3d-cofold-smooth-f4": dict(dim=3, cells=(16, 12, 12), covariance="matern32", corr_length=0.25,
+                                embedding_factor=4, periodization="cofold", sigmoid="smooth",
+                                cofold_max_factor=3.0, approximate=True),
+    "2d-cofold-geo-r2c-f4": dict(dim=2, cells=(24, 20), covariance="exponential",
+                                 corr_length=(0.4, 0.1, -0.1, 0.3), anisotropy="geometric", embedding_factor=4,
+                                 periodization="cofold", cofold_recursions=3, approximate=True),
     # tori whose lengths have prime factors above 13: Bluestein transforms
     "2d-exp-prime": dict(dim=2, cells=(131, 97), covariance="exponential", corr_length=0.1),
     "3d-sph-prime": dict(dim=3, cells=(17, 19, 23), covariance="spherical", corr_length=0.2),

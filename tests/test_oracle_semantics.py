@@ -260,3 +260,115 @@ def test_fold_periodization_keeps_domain_and_stretches_beyond(oracle):
         assert np.abs(a[inside] - b[inside]).max() < 1e-14
         assert (b[~inside] >= a[~inside] - 1e-15).all()
         assert np.abs(a[~inside] - b[~inside]).max() > 1e-3
+
+
+def _sigmoid_ref(kind, one, zero, x, rec):
+    """SmoothstepSigmoid / SmoothSigmoid (covariance.hh:147-287), scalar restatement."""
+    ax = abs(x)
+    if kind == "smooth":
+        if ax < one:
+            return 1.0
+        if ax > zero:
+            return 0.0
+        x1, x2 = (zero - ax) / (zero - one), (ax - one) / (zero - one)
+        t1 = np.exp(-1.0 / x1) if x1 > 0 else 0.0
+        t2 = np.exp(-1.0 / x2) if x2 > 0 else 0.0
+        return t1 / (t1 + t2)
+    x1 = 1.0 if ax < one else (0.0 if ax > zero else (zero - ax) / (zero - one))
+    x2 = 2.0 * x1 - 1.0
+    norm, add, out = 1.0, 1.0, 1.0
+    for i in range(1, rec + 1):
+        out *= 2.0 * i
+        add *= 1 - x2 * x2
+        out += add
+        out /= 2.0 * i + 1.0
+        norm *= 2.0 * i / (2.0 * i + 1.0)
+    return (out * x2 / norm + 1.0) / 2.0
+
+
+def _cofold_numpy(oracle, desc, base_values, sig, rec, max_factor):
+    """modifyMatrixEntriesWithCofold (matrix.hh:905-1013) restated over the oracle's classical
+    fill, with scipy's adaptive quadrature for the sigmoid integrals."""
+    from scipy.integrate import quad
+    import pfb200
+    g = oracle.resolve(desc)
+    if g.matrix_backend == pfb200.MATRIX_DCT:
+        cells = [g.T[i] // 2 + 1 for i in range(g.dim)]
+    elif g.matrix_backend == pfb200.MATRIX_R2C:
+        cells = [2 * (g.T[0] // 2 + 1)] + [g.T[i] for i in range(1, g.dim)]
+    else:
+        cells = [g.T[i] for i in range(g.dim)]
+    idx = np.arange(base_values.size)
+    coords, r = [], idx.copy()
+    for i in range(g.dim):
+        c = (r % cells[i]).astype(np.float64) * g.h[i]
+        r //= cells[i]
+        half, wrap = 0.5 * g.ext[i] * g.factor, g.ext[i] * g.factor
+        coords.append(np.where(c > half, c - wrap, c))
+    norm = np.max(np.stack([np.abs(c) / g.ext[i] for i, c in enumerate(coords)]), axis=0)
+    border = np.zeros(idx.size, bool)
+    for i, c in enumerate(coords):
+        border |= 0.5 * g.ext[i] * g.factor - np.abs(c) < g.ext[i] / g.T[i]
+    inside = norm <= 1.0
+    min_c = base_values[inside].min()
+    alpha = base_values[~inside & border].max()
+    beta = min(max_factor * alpha, min_c)
+    f = lambda t: _sigmoid_ref(sig, 0.0, beta - alpha, beta - t, rec)  # noqa: E731
+    offset = beta - quad(f, alpha, beta, epsabs=1e-14, epsrel=1e-12)[0]
+    out = base_values.copy()
+    for k in np.nonzero(~inside)[0]:
+        x = base_values[k]
+        if x < alpha:
+            out[k] = offset
+        elif x < beta:
+            out[k] = quad(f, alpha, x, epsabs=1e-14, epsrel=1e-12)[0] + offset
+    return out, alpha, beta
+
+
+@pytest.mark.parametrize("case", [
+    dict(kw=dict(dim=2, cells=(16, 12), covariance="exponential", corr_length=0.5, embedding_factor=3),
+         sig="smoothstep", rec=1, mf=5.0),
+    dict(kw=dict(dim=3, cells=(8, 6, 4), covariance="matern32", corr_length=0.3, embedding_factor=4),
+         sig="smooth", rec=1, mf=5.0),
+    dict(kw=dict(dim=2, cells=(12, 10), covariance="exponential", corr_length=(0.4, 0.1, -0.1, 0.3),
+                 anisotropy="geometric", embedding_factor=4), sig="smoothstep", rec=3, mf=3.0),
+    # factor 3 in 3D: the domain corner (radius sqrt 3) lies beyond the border (1.5), so
+    # beta < alpha and every value below alpha becomes beta (the reference's arithmetic)
+    dict(kw=dict(dim=3, cells=(8, 6, 4), covariance="matern32", corr_length=(0.3, 0.2, 0.25),
+                 anisotropy="axiparallel", embedding_factor=3), sig="smooth", rec=1, mf=5.0, inverted=True),
+])
+def test_cofold_periodization_matches_restatement(oracle, case):
+    """embedding.periodization = cofold: the oracle's C restatement against an independent
+    numpy/scipy restatement over the classical fill (DCT matrix, and R2C with its padding)."""
+    import pfb200
+    base = pfb200.make_desc(**case["kw"])
+    cof = pfb200.make_desc(**case["kw"], periodization="cofold", sigmoid=case["sig"],
+                           cofold_recursions=case["rec"], cofold_max_factor=case["mf"])
+    a = oracle.fill_matrix(base)
+    b = oracle.fill_matrix(cof)
+    want, alpha, beta = _cofold_numpy(oracle, cof, a, case["sig"], case["rec"], case["mf"])
+    assert (alpha > beta) == case.get("inverted", False)
+    assert np.abs(b - want).max() <= 1e-12 * np.abs(a).max()
+    assert np.abs(a - b).max() > 1e-6 * np.abs(a).max()
+
+
+def test_cofold_keeps_domain_values_and_lifts_the_rest(oracle):
+    """Cofold never changes a value within the domain's extent (norm <= 1) and never lowers
+    a value beyond it: values below the border maximum alpha are lifted to the offset."""
+    import pfb200
+    kw = dict(dim=2, cells=(16, 12), covariance="exponential", corr_length=0.5, embedding_factor=3)
+    g = oracle.resolve(pfb200.make_desc(**kw))
+    a = oracle.fill_matrix(pfb200.make_desc(**kw))
+    b = oracle.fill_matrix(pfb200.make_desc(**kw, periodization="cofold"))
+    j1, j0 = np.meshgrid(np.arange(g.T[1] // 2 + 1), np.arange(g.T[0] // 2 + 1), indexing="ij")
+    norm = np.maximum(j0 * g.h[0] / g.ext[0], j1 * g.h[1] / g.ext[1]).ravel()
+    inside = norm <= 1.0
+    assert np.array_equal(a[inside], b[inside])
+    assert (b[~inside] >= a[~inside]).all()
+
+
+def test_cofold_rejects_negative_recursions(oracle):
+    import pfb200
+    d = pfb200.make_desc(dim=2, cells=(8, 8), periodization="cofold", cofold_recursions=-1)
+    with pytest.raises(ValueError, match="cofoldRecursions"):
+        oracle.resolve(d)
