@@ -48,6 +48,25 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def realization_work(cells, torus):
+    """Compulsory HBM bytes and FFT flops of one FP32 realization with in-register noise
+    (per-unit figures of the measurement plan): bytes = sqrt(lambda) on the prod(T/2+1) DCT
+    cells (FP32) + the field (FP32); flops = 2.5 N log2 N for the real 3D transform of the
+    torus, N = prod(T).  Also the flops of each pass of the pruned schedule the library runs
+    (complex pencils: 5 L log2 L; the final complex-to-real rows: 2.5 L log2 L)."""
+    import math
+    t0, t1, t2 = torus
+    n0, n1, n2 = cells
+    N = t0 * t1 * t2
+    sq = (t0 // 2 + 1) * (t1 // 2 + 1) * (t2 // 2 + 1) * 4
+    out = n0 * n1 * n2 * 4
+    c = lambda L: 5.0 * L * math.log2(L)  # noqa: E731
+    passes = {"gen_noise_last": (t0 // 2 + 1) * t1 * c(t2),   # last axis, every pencil of the half spectrum
+              "gen_c2c_d1": (t0 // 2 + 1) * n2 * c(t1),       # axis 1 on the n2 kept planes
+              "gen_c2r_d0": n1 * n2 * 0.5 * c(t0)}            # complex-to-real rows of the kept cells
+    return {"compulsory_bytes": sq + out, "flops": 2.5 * N * math.log2(N), "pass_flops": passes}
+
+
 def ncu_traffic():
     """per-launch DRAM bytes of each kernel from the committed ncu summary, if any"""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
@@ -171,6 +190,7 @@ def run_b200(args):
     P.set_stream(stream.cuda_stream)
     P.spectrum_build()
     P.autotune()  # measured planning of the realization passes (outside the timed region)
+    fpeaks = pfb200.measure_peaks(local) if rank == 0 else None  # CUDA-core FMA peaks (untimed)
     n = P.info.domain_size
     out = torch.empty(n, dtype=torch.float32, device=dev)
     # the K timed realizations go through one pf_generate_batch call, which alternates them
@@ -238,6 +258,26 @@ def run_b200(args):
                     "traffic": tr, "algorithmic_bytes_per_launch": bytes_per, "avg_launch_ms": avg_ms,
                     "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()}
                                 for r in prof]}
+        work = realization_work(WORKLOAD["cells"], CONFIG["torus"])
+        f32peak = max(fpeaks["fp32_ffma_tflops"], fpeaks["fp32_ffma2_tflops"])
+        real_s = ms / args.steps / 1e3
+        compute = {
+            "fp32_peak_tflops": round(f32peak, 1), "fp32_ffma_tflops": round(fpeaks["fp32_ffma_tflops"], 1),
+            "fp64_peak_tflops": round(fpeaks["fp64_dfma_tflops"], 1),
+            "peak_source": "in-register FMA microbenchmark (pf_measure_peaks) on this GPU before the timed region",
+            "realization": {
+                "compulsory_bytes": work["compulsory_bytes"],
+                "hbm_gbs": round(work["compulsory_bytes"] / real_s / 1e9, 1),
+                "hbm_frac": round(work["compulsory_bytes"] / real_s / 1e9 / peak, 4),
+                "flops": work["flops"], "tflops": round(work["flops"] / real_s / 1e12, 2),
+                "fp32_frac": round(work["flops"] / real_s / 1e12 / f32peak, 4),
+                "note": "per realization of the timed (pipelined) region: sqrt(lambda) FP32 on the DCT "
+                        "cells + FP32 field; 2.5 N log2 N flops of the full real 3D transform"}}
+        if dom and dom["name"] in work["pass_flops"]:
+            pf = work["pass_flops"][dom["name"]]
+            tfl = pf / (avg_ms / 1e3) / 1e12
+            compute["dominant_kernel"] = {"kernel": dom["name"], "flops": pf, "tflops": round(tfl, 2),
+                                          "fp32_frac": round(tfl / f32peak, 4)}
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             threads = os.cpu_count() or 1
@@ -255,7 +295,7 @@ def run_b200(args):
                         "note": f"pf_generate_batch(seed, count={ke}, pinned host out): seed passed by value, "
                                 "every realization copied to the host inside the region while the next one is "
                                 "computed (wall clock)"},
-                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+                "gpu_launches": launches, "roofline": roof, "compute": compute, "cpu_baseline": cpu,
                 "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"],
                            "reasons": clocks["reasons"]}}
         print(json.dumps(line), flush=True)

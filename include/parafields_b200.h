@@ -392,6 +392,19 @@ typedef struct pf_kernel_time {
 } pf_kernel_time;
 pf_status pf_profile_read(pf_plan* plan, pf_kernel_time* out, int32_t cap, int32_t* count);
 
+/* CUDA-core arithmetic peaks of `device` (B200 extension, no reference counterpart): FP32
+ * FFMA, paired FP32 FFMA2 and FP64 DFMA throughput from an in-register FMA microbenchmark
+ * (best of 3 timed launches after one warm-up), the denominators of compute fractions. */
+typedef struct pf_peaks {
+  double fp32_ffma_tflops;
+  double fp32_ffma2_tflops;
+  double fp64_dfma_tflops;
+  double sm_clock_mhz; /* the device's nominal maximum SM clock */
+  int32_t sms;
+  int32_t pad_;
+} pf_peaks;
+pf_status pf_measure_peaks(int32_t device, pf_peaks* out);
+
 /* Number of kernel launches issued by this plan since creation. */
 uint64_t pf_launch_count(const pf_plan* plan);
 

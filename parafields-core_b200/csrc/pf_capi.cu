@@ -1958,3 +1958,4 @@ extern "C" pf_status pf_matvec_static(pf_plan* P, int32_t op, const double* in, 
 
 #include "pf_ensemble.inc"
 #include "pf_tune.inc"
+#include "pf_peaks.inc"

@@ -149,6 +149,12 @@ def make_desc(dim=2, cells=(16, 16), extensions=None, covariance="exponential", 
 _lib = None
 
 
+class Peaks(C.Structure):
+    _fields_ = [("fp32_ffma_tflops", C.c_double), ("fp32_ffma2_tflops", C.c_double),
+                ("fp64_dfma_tflops", C.c_double), ("sm_clock_mhz", C.c_double), ("sms", C.c_int32),
+                ("pad_", C.c_int32)]
+
+
 def lib():
     """Loads libpfcuda.so (raises if it was not built)."""
     global _lib
@@ -197,6 +203,7 @@ def lib():
         "pf_wisdom_export": (i32, [C.c_char_p, u64, C.POINTER(u64)]),
         "pf_wisdom_import": (i32, [C.c_char_p]),
         "pf_wisdom_forget": (None, []),
+        "pf_measure_peaks": (i32, [i32, C.POINTER(Peaks)]),
         "pf_last_error_string": (C.c_char_p, []),
         "pf_version": (C.c_char_p, []),
     }
@@ -474,3 +481,11 @@ def wisdom_import(text):
 
 def wisdom_forget():
     lib().pf_wisdom_forget()
+
+
+def measure_peaks(device=0):
+    """CUDA-core FP32 (FFMA, FFMA2) and FP64 (DFMA) throughput of `device` in TFLOP/s."""
+    p = Peaks()
+    _check(lib().pf_measure_peaks(device, C.byref(p)))
+    return {"fp32_ffma_tflops": p.fp32_ffma_tflops, "fp32_ffma2_tflops": p.fp32_ffma2_tflops,
+            "fp64_dfma_tflops": p.fp64_dfma_tflops, "sm_clock_mhz": p.sm_clock_mhz, "sms": p.sms}

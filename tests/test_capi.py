@@ -32,15 +32,17 @@ def test_library_exports_every_declared_symbol():
 def test_struct_layouts_match_c(tmp_path):
     src = tmp_path / "sz.c"
     src.write_text('#include "parafields_b200.h"\n#include <stdio.h>\n#include <stddef.h>\n'
-                   'int main(){printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(pf_field_desc), '
+                   'int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(pf_field_desc), '
                    'sizeof(pf_eig_stats), sizeof(pf_plan_info), sizeof(pf_cg_opts), sizeof(pf_cg_report), '
-                   'sizeof(pf_kernel_time), offsetof(pf_field_desc, boxcox_lambda));return 0;}\n')
+                   'sizeof(pf_kernel_time), offsetof(pf_field_desc, boxcox_lambda), '
+                   'offsetof(pf_field_desc, cofold_max_factor), sizeof(pf_peaks));return 0;}\n')
     exe = tmp_path / "sz"
     subprocess.run(["/usr/bin/gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     exp = [C.sizeof(pfb200.FieldDesc), C.sizeof(pfb200.EigStats), C.sizeof(pfb200.PlanInfo),
            C.sizeof(pfb200.CgOpts), C.sizeof(pfb200.CgReport), C.sizeof(pfb200.KernelTime),
-           pfb200.FieldDesc.boxcox_lambda.offset]
+           pfb200.FieldDesc.boxcox_lambda.offset, pfb200.FieldDesc.cofold_max_factor.offset,
+           C.sizeof(pfb200.Peaks)]
     assert got == exp
 
 
