@@ -296,6 +296,27 @@ __device__ __forceinline__ float2 box_muller_fast(uint32_t a, uint32_t b) {
   return make_float2(rad * c, rad * s);
 }
 
+// Box-Muller for pencils A and B at once: (a, b) of pencil A and (c, d) of pencil B give
+// the normal pairs (re, im) of both in the pair layout re = (Re A, Re B), im = (Im A, Im B);
+// the same operations and rounding as box_muller_fast, the products issued as FMUL2/FFMA2
+__device__ __forceinline__ P2 box_muller_pair(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  const float2 u1 = f2fma(make_float2(__uint2float_rn(a), __uint2float_rn(c)),
+                          make_float2(2.3283064365386963e-10f, 2.3283064365386963e-10f),
+                          make_float2(1.1641532182693481e-10f, 1.1641532182693481e-10f));
+  const float2 x2 = f2mul(make_float2(__log2f(u1.x), __log2f(u1.y)),
+                          make_float2(-1.3862943611198906f, -1.3862943611198906f));
+  const float2 x = make_float2(fmaxf(x2.x, 1e-30f), fmaxf(x2.y, 1e-30f));
+  const float2 rad = f2mul(x, make_float2(rsqrtf(x.x), rsqrtf(x.y)));
+  const float2 u2 = f2add(make_float2(__uint_as_float(0x3f800000u | (b >> 9)), __uint_as_float(0x3f800000u | (d >> 9))),
+                          make_float2(-1.0f, -1.0f));
+  const float2 ang = f2fma(make_float2(6.283185307179586f, 6.283185307179586f), u2,
+                           make_float2(-3.141592653589793f, -3.141592653589793f));
+  float sA, cA, sB, cB;
+  __sincosf(ang.x, &sA, &cA);
+  __sincosf(ang.y, &sB, &cB);
+  return {f2mul(rad, make_float2(cA, cB)), f2mul(rad, make_float2(sA, sB))};
+}
+
 template <int DIM, int LAYOUT, bool TRANSP>
 struct P2Noise {
   // LAYOUT: 1 = DCT prod(T/2+1) eigenvalues (mirrored lookup), 0 = R2C half spectrum,
@@ -341,6 +362,84 @@ struct P2Noise {
     o.re = f2mul(make_float2(sA, sB), make_float2(rA.x, rB.x));
     o.im = make_float2(scA ? 0.f : sA * rA.y, scB ? 0.f : sB * rB.y);
     return o;
+  }
+  // Per-tile part of the counter-noise lookups (the pass axis is the last torus axis, so its
+  // length is the transform length L): for elements j < L/2 and j + L/2 of pencils
+  // (k0, k0+1) at outer index k1, the stored index is si0 + sstride * kl, the eigenvalue
+  // index li0 + lstride * m(kl) with m(kl) = kl, or min(kl, L - kl) for the DCT layout, and
+  // the self-conjugate rule reduces to (row part) && j == 0.  One bounds check covers the
+  // tile.
+  struct Tile {
+    unsigned si0, sstride, li0, lstride;
+    bool vb, ok, scA, scB;
+  };
+  template <int L>
+  __device__ __forceinline__ Tile tile(int p, int o, unsigned& bad) const {
+    Tile t;
+    const int k0 = p, k1 = DIM == 3 ? o : 0;
+    if (DIM == 2) {
+      t.si0 = (unsigned)k0;
+      t.sstride = (unsigned)T0c;
+    } else if (TRANSP) {
+      t.si0 = (unsigned)k0 + (unsigned)T0c * (unsigned)ext2 * (unsigned)k1;
+      t.sstride = (unsigned)T0c;
+    } else {
+      t.si0 = (unsigned)k0 + (unsigned)T0c * (unsigned)k1;
+      t.sstride = (unsigned)T0c * (unsigned)ext1;
+    }
+    if (LAYOUT == 1) {
+      const int m1 = k1 <= ext1 / 2 ? k1 : ext1 - k1;
+      t.li0 = (unsigned)k0 + (DIM == 3 ? (unsigned)D0 * (unsigned)m1 : 0u);
+      t.lstride = DIM == 3 ? (unsigned)D0 * (unsigned)D1 : (unsigned)D0;
+    } else if (LAYOUT == 2) {
+      t.li0 = (unsigned)k0 + (DIM == 3 ? (unsigned)ext0 * (unsigned)k1 : 0u);
+      t.lstride = DIM == 3 ? (unsigned)ext0 * (unsigned)ext1 : (unsigned)ext0;
+    } else {
+      t.li0 = (unsigned)k0 + (DIM == 3 ? (unsigned)T0c * (unsigned)k1 : 0u);
+      t.lstride = DIM == 3 ? (unsigned)T0c * (unsigned)ext1 : (unsigned)T0c;
+    }
+    t.vb = k0 + 1 < np;
+    const unsigned mmax = LAYOUT == 1 ? (unsigned)(L / 2) : (unsigned)(L - 1);
+    const unsigned long long top = (unsigned long long)t.li0 + (unsigned long long)t.lstride * mmax + (t.vb ? 1u : 0u);
+    t.ok = p < np && top < (unsigned long long)nsq;
+    bad |= (unsigned)(p < np && !t.ok);
+    const bool sc1 = DIM < 3 || k1 == 0 || 2 * k1 == ext1;
+    t.scA = sc1 && (k0 == 0 || 2 * k0 == ext0);
+    t.scB = sc1 && 2 * (k0 + 1) == ext0;
+    return t;
+  }
+  // normals z (pair layout) times (lambda A, lambda B) of eigenvalue index li, with the
+  // self-conjugate rule (factor 1 and zero imaginary part) at the rows' first element
+  __device__ __forceinline__ P2 scale_t(const Tile& t, unsigned li, bool first, const P2& z) const {
+    const float lA = sq[li];
+    const float lB = t.vb ? sq[li + 1] : 0.f;
+    const bool scA = t.scA && first, scB = t.scB && first;
+    const float h = 0.70710678118654752f;
+    const float2 s = f2mul(make_float2(lA, lB), make_float2(scA ? 1.f : h, scB ? 1.f : h));
+    P2 o;
+    o.re = f2mul(s, z.re);
+    o.im = f2mul(s, z.im);
+    if (scA) o.im.x = 0.f;
+    if (scB) o.im.y = 0.f;
+    return o;
+  }
+  // counter noise of elements j < L/2 and j + L/2 of the tile's pencil pair
+  template <int L>
+  __device__ __forceinline__ void load2t(const Tile& t, int j, P2& x0, P2& x1) const {
+    if (!t.ok) {
+      x0 = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+      x1 = x0;
+      return;
+    }
+    constexpr int h = L / 2;
+    const unsigned si = t.si0 + t.sstride * (unsigned)j;
+    const unsigned ep = epoch ? __ldg(epoch) : 0u;
+    const uint4 cA = philox_rk(make_uint4(si, 0u, 0x70616972u, ep), keys);
+    const uint4 cB = philox_rk(make_uint4(si + 1u, 0u, 0x70616972u, ep), keys);
+    const P2 z0 = box_muller_pair(cA.x, cA.y, cB.x, cB.y), z1 = box_muller_pair(cA.z, cA.w, cB.z, cB.w);
+    const unsigned m1 = LAYOUT == 1 ? (unsigned)(h - j) : (unsigned)(j + h);
+    x0 = scale_t(t, t.li0 + t.lstride * (unsigned)j, j == 0, z0);
+    x1 = scale_t(t, t.li0 + t.lstride * m1, j == 0, z1);
   }
   // elements j and j + L/2 of pencils (p, p+1); pencil = k0, outer = k1
   template <int L>
@@ -403,8 +502,14 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
     const int o = (int)(tile / tpo);
     const int p = (int)(tile - (long long)o * tpo) * G::NP + 2 * q;
     P2 v[8];
+    if (ld.noise) {  // noise buffer in the reference's draw order
 #pragma unroll
-    for (int r = 0; r < 4; r++) ld.template load2<L>(p, u + r * G::TP, o, v[r], v[r + 4], bad);
+      for (int r = 0; r < 4; r++) ld.template load2<L>(p, u + r * G::TP, o, v[r], v[r + 4], bad);
+    } else {  // counter-based noise: index arithmetic and bounds check once per tile
+      const auto t = ld.template tile<L>(p, o, bad);
+#pragma unroll
+      for (int r = 0; r < 4; r++) ld.template load2t<L>(t, u + r * G::TP, v[r], v[r + 4]);
+    }
     p2_transform<L, +1>(v, buf, tw, u, q, [&](int j, const P2& x) {
       if (j < Lout) st.store(p, j, o, x, bad);
     });
