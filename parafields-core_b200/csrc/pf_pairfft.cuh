@@ -213,14 +213,24 @@ struct P2ArrLoad {
   unsigned n;                 // complex elements in the buffer
   int Lin;
   int np;
-  __device__ __forceinline__ P2 load(int p, int j, int o, unsigned& bad) const {
-    const unsigned i = (unsigned)p + (unsigned)j * jstride + (unsigned)o * ostride;
-    const bool want = j < Lin && p < np;
-    const bool ok = want && i + 1 < n;
-    bad |= (unsigned)(want && !ok);
+  // per-tile part of the loads of pencils (p, p+1) at outer index o, elements j < Lin
+  struct Tile {
+    unsigned base;
+    bool two, ok;
+  };
+  __device__ __forceinline__ Tile tile(int p, int o, unsigned& bad) const {
+    Tile t;
+    t.base = (unsigned)p + (unsigned)o * ostride;
+    t.two = p + 1 < np;
+    const unsigned long long top = (unsigned long long)t.base + (unsigned long long)(Lin - 1) * jstride + 1u;
+    t.ok = p < np && Lin > 0 && top < (unsigned long long)n;
+    bad |= (unsigned)(p < np && Lin > 0 && !t.ok);
+    return t;
+  }
+  __device__ __forceinline__ P2 load_t(const Tile& t, int j) const {
     float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (ok) s = ptr[i >> 1];
-    if (p + 1 >= np) {
+    if (t.ok && j < Lin) s = ptr[(t.base + (unsigned)j * jstride) >> 1];
+    if (!t.two) {
       s.z = 0.f;
       s.w = 0.f;
     }
@@ -233,14 +243,26 @@ struct P2ArrStore {
   unsigned jstride, ostride;
   unsigned n;
   int np;
-  __device__ __forceinline__ void store(int p, int j, int o, const P2& v, unsigned& bad) const {
-    if (p >= np) return;
-    const unsigned i = (unsigned)p + (unsigned)j * jstride + (unsigned)o * ostride;
-    const bool two = p + 1 < np;
-    const bool ok = i + (two ? 1u : 0u) < n;
-    bad |= (unsigned)!ok;
-    if (!ok) return;
-    if (two)
+  // per-tile part of the stores of pencils (p, p+1) at outer index o, elements j < Lout:
+  // base index, whether pencil p+1 exists, and one bounds check for the whole tile
+  struct Tile {
+    unsigned base;
+    bool two, ok;
+  };
+  __device__ __forceinline__ Tile tile(int p, int o, int Lout, unsigned& bad) const {
+    Tile t;
+    t.base = (unsigned)p + (unsigned)o * ostride;
+    t.two = p + 1 < np;
+    const unsigned long long top =
+        (unsigned long long)t.base + (unsigned long long)(Lout - 1) * jstride + (t.two ? 1u : 0u);
+    t.ok = p < np && Lout > 0 && top < (unsigned long long)n;
+    bad |= (unsigned)(p < np && Lout > 0 && !t.ok);
+    return t;
+  }
+  __device__ __forceinline__ void store_t(const Tile& t, int j, const P2& v) const {
+    if (!t.ok) return;
+    const unsigned i = t.base + (unsigned)j * jstride;
+    if (t.two)
       ptr[i >> 1] = make_float4(v.re.x, v.im.x, v.re.y, v.im.y);
     else
       reinterpret_cast<float2*>(ptr)[i] = make_float2(v.re.x, v.im.x);
@@ -370,7 +392,7 @@ struct P2Noise {
   // the self-conjugate rule reduces to (row part) && j == 0.  One bounds check covers the
   // tile.
   struct Tile {
-    unsigned si0, sstride, li0, lstride;
+    unsigned si0, sstride, li0, lstride, ep;
     bool vb, ok, scA, scB;
   };
   template <int L>
@@ -406,6 +428,7 @@ struct P2Noise {
     const bool sc1 = DIM < 3 || k1 == 0 || 2 * k1 == ext1;
     t.scA = sc1 && (k0 == 0 || 2 * k0 == ext0);
     t.scB = sc1 && 2 * (k0 + 1) == ext0;
+    t.ep = epoch ? __ldg(epoch) : 0u;
     return t;
   }
   // normals z (pair layout) times (lambda A, lambda B) of eigenvalue index li, with the
@@ -433,9 +456,8 @@ struct P2Noise {
     }
     constexpr int h = L / 2;
     const unsigned si = t.si0 + t.sstride * (unsigned)j;
-    const unsigned ep = epoch ? __ldg(epoch) : 0u;
-    const uint4 cA = philox_rk(make_uint4(si, 0u, 0x70616972u, ep), keys);
-    const uint4 cB = philox_rk(make_uint4(si + 1u, 0u, 0x70616972u, ep), keys);
+    const uint4 cA = philox_rk(make_uint4(si, 0u, 0x70616972u, t.ep), keys);
+    const uint4 cB = philox_rk(make_uint4(si + 1u, 0u, 0x70616972u, t.ep), keys);
     const P2 z0 = box_muller_pair(cA.x, cA.y, cB.x, cB.y), z1 = box_muller_pair(cA.z, cA.w, cB.z, cB.w);
     const unsigned m1 = LAYOUT == 1 ? (unsigned)(h - j) : (unsigned)(j + h);
     x0 = scale_t(t, t.li0 + t.lstride * (unsigned)j, j == 0, z0);
@@ -510,8 +532,9 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
 #pragma unroll
       for (int r = 0; r < 4; r++) ld.template load2t<L>(t, u + r * G::TP, v[r], v[r + 4]);
     }
+    const P2ArrStore::Tile so = st.tile(p, o, Lout, bad);
     p2_transform<L, +1>(v, buf, tw, u, q, [&](int j, const P2& x) {
-      if (j < Lout) st.store(p, j, o, x, bad);
+      if (j < Lout) st.store_t(so, j, x);
     });
   }
   p2_report(bad);
@@ -535,10 +558,12 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
     const int o = (int)(tile / tpo);
     const int p = (int)(tile - (long long)o * tpo) * G::NP + 2 * q;
     P2 v[8];
+    const P2ArrLoad::Tile lt = ld.tile(p, o, bad);
 #pragma unroll
-    for (int r = 0; r < 8; r++) v[r] = ld.load(p, u + r * G::TP, o, bad);
+    for (int r = 0; r < 8; r++) v[r] = ld.load_t(lt, u + r * G::TP);
+    const P2ArrStore::Tile so = st.tile(p, o, Lout, bad);
     p2_transform<L, S>(v, buf, tw, u, q, [&](int j, const P2& x) {
-      if (j < Lout) st.store(p, j, o, x, bad);
+      if (j < Lout) st.store_t(so, j, x);
     });
   }
   p2_report(bad);
