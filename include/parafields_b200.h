@@ -48,7 +48,8 @@ typedef enum pf_status {
   PF_ERR_NOT_CONVERGED = 5, /* CG hit its iteration cap without the requested residual */
   PF_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up */
   PF_ERR_STATE = 7,         /* call order violated (e.g. spectrum missing) */
-  PF_ERR_ARG = 8            /* null pointer / size mismatch */
+  PF_ERR_ARG = 8,           /* null pointer / size mismatch */
+  PF_ERR_IO = 9             /* a field file is missing, unreadable or not of the expected shape */
 } pf_status;
 
 /* stochastic.covariance (matrix.hh:232-260) */
@@ -391,6 +392,19 @@ typedef struct pf_kernel_time {
   double bytes;  /* algorithmic bytes moved by all launches (reads + writes) */
 } pf_kernel_time;
 pf_status pf_profile_read(pf_plan* plan, pf_kernel_time* out, int32_t cap, int32_t* count);
+
+/* StochasticPart::writeToFile (stochastic.hh:273-294, io.hh:170-349): the field in `data`
+ * (host or device memory per `mem`, FP64 or FP32 per `precision`, dimension 0 fastest) to
+ * "<base>.stoch.h5" (dataset /stochastic, IEEE F64LE, dimensions the cells in reverse order)
+ * and "<base>.xdmf".  The HDF5 file is written without libhdf5 (version 0 superblock,
+ * symbol-table root group, contiguous dataset). */
+pf_status pf_field_write(const char* base, int32_t dim, const int32_t* cells, const double* extensions,
+                         const void* data, int32_t precision, int32_t mem);
+/* StochasticPart(traits, fileName) (stochastic.hh:80-110): "<base>.stoch.h5" into `data`
+ * (host or device, FP64 or FP32); PF_ERR_IO when the file is missing ("File is missing: ...")
+ * or its dataset does not hold the cells. */
+pf_status pf_field_read(const char* base, int32_t dim, const int32_t* cells, void* data, int32_t precision,
+                        int32_t mem);
 
 /* CUDA-core arithmetic peaks of `device` (B200 extension, no reference counterpart): FP32
  * FFMA, paired FP32 FFMA2 and FP64 DFMA throughput from an in-register FMA microbenchmark

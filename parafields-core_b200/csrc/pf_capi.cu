@@ -24,6 +24,7 @@
 #include "pf_fastfft.cuh"
 #include "pf_pairfft.cuh"
 #include "pf_learned.cuh"
+#include "../include/parafields_b200/fieldio.hh"
 
 using namespace pf;
 
@@ -1959,3 +1960,4 @@ extern "C" pf_status pf_matvec_static(pf_plan* P, int32_t op, const double* in, 
 #include "pf_ensemble.inc"
 #include "pf_tune.inc"
 #include "pf_peaks.inc"
+#include "pf_io.inc"

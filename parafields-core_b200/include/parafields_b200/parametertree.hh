@@ -8,6 +8,7 @@
 #include <cctype>
 #include <fstream>
 #include <map>
+#include <ostream>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -57,6 +58,23 @@ class ParameterTree {
       std::string val = trim(line.substr(eq + 1));
       if (val.size() >= 2 && val.front() == '"' && val.back() == '"') val = val.substr(1, val.size() - 2);
       values_[prefix + trim(line.substr(0, eq))] = val;
+    }
+  }
+
+  // Dune::ParameterTree::report layout: keys without a section as key = "value", then one
+  // "[ section ]" block per section (sorted) with its keys relative to it
+  void report(std::ostream& out) const {
+    std::map<std::string, std::map<std::string, std::string>> sections;
+    for (const auto& kv : values_) {
+      const auto dot = kv.first.rfind('.');
+      if (dot == std::string::npos)
+        sections[""][kv.first] = kv.second;
+      else
+        sections[kv.first.substr(0, dot)][kv.first.substr(dot + 1)] = kv.second;
+    }
+    for (const auto& sec : sections) {
+      if (!sec.first.empty()) out << "[ " << sec.first << " ]\n";
+      for (const auto& kv : sec.second) out << kv.first << " = \"" << kv.second << "\"\n";
     }
   }
 

@@ -19,6 +19,7 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <fstream>
 #include <memory>
 #include <random>
 #include <stdexcept>
@@ -26,6 +27,7 @@
 #include <vector>
 
 #include "../../../include/parafields_b200.h"
+#include "fieldio.hh"
 #include "parametertree.hh"
 
 namespace parafields_b200 {
@@ -365,7 +367,36 @@ class RandomField {
     dataCells_ = cells_;
   }
 
+  static ParameterTree configFromFile(const std::string& fileName) {
+    ParameterTree c;
+    c.readIniFile(fileName + ".field");
+    return c;
+  }
+
  public:
+  // randomfield.hh:135-172 (with a file name: stochastic.hh:80-110, the field is read from
+  // "<fileName>.stoch.h5"; the cached products are then invalid)
+  RandomField(const ParameterTree& config, const std::string& fileName) : RandomField(config) {
+    if (fileName.empty()) return;
+    const std::vector<double> v = readStochastic(fileName, dim, cells_.data());
+    data_.assign(v.begin(), v.end());
+    invMatvecValid_ = invRootMatvecValid_ = false;
+  }
+  // randomfield.hh:192-230: configuration from "<fileName>.field", field from
+  // "<fileName>.stoch.h5"
+  explicit RandomField(const std::string& fileName) : RandomField(configFromFile(fileName), fileName) {}
+
+  // randomfield.hh:706-713 (trend components are not part of this path): the field to
+  // "<fileName>.stoch.h5" and "<fileName>.xdmf", the configuration to "<fileName>.field"
+  void writeToFile(const std::string& fileName) const {
+    if (dataCells_ != cells_) throw std::runtime_error{"writeToFile: call refine() or coarsen() first"};
+    writeStochastic(fileName, dim, cells_.data(), data_.data());
+    writeXdmf(fileName, dim, cells_.data(), ext_.data());
+    std::ofstream file(fileName + ".field", std::ofstream::trunc);
+    if (!file) throw std::runtime_error{"cannot create " + fileName + ".field"};
+    config_.report(file);
+  }
+
   explicit RandomField(const ParameterTree& config)
       : config_(config),
         desc_(descFromConfig<dim, RF>(config)),

@@ -20,7 +20,7 @@ LIB_PATH = os.environ.get("PFB200_LIB", os.path.join(HERE, "lib", "libpfcuda.so"
 
 # --- enums (include/parafields_b200.h) ---------------------------------------
 PF_OK, PF_ERR_NEG_EIGEN, PF_ERR_CONFIG, PF_ERR_OOM, PF_ERR_CUDA = 0, 1, 2, 3, 4
-PF_ERR_NOT_CONVERGED, PF_ERR_TIMEOUT, PF_ERR_STATE, PF_ERR_ARG = 5, 6, 7, 8
+PF_ERR_NOT_CONVERGED, PF_ERR_TIMEOUT, PF_ERR_STATE, PF_ERR_ARG, PF_ERR_IO = 5, 6, 7, 8, 9
 
 COVARIANCES = {
     "exponential": 0, "gaussian": 1, "spherical": 2, "separableExponential": 3,
@@ -204,6 +204,8 @@ def lib():
         "pf_wisdom_import": (i32, [C.c_char_p]),
         "pf_wisdom_forget": (None, []),
         "pf_measure_peaks": (i32, [i32, C.POINTER(Peaks)]),
+        "pf_field_write": (i32, [C.c_char_p, i32, C.POINTER(i32), C.POINTER(C.c_double), vp, i32, i32]),
+        "pf_field_read": (i32, [C.c_char_p, i32, C.POINTER(i32), vp, i32, i32]),
         "pf_last_error_string": (C.c_char_p, []),
         "pf_version": (C.c_char_p, []),
     }
@@ -489,3 +491,27 @@ def measure_peaks(device=0):
     _check(lib().pf_measure_peaks(device, C.byref(p)))
     return {"fp32_ffma_tflops": p.fp32_ffma_tflops, "fp32_ffma2_tflops": p.fp32_ffma2_tflops,
             "fp64_dfma_tflops": p.fp64_dfma_tflops, "sm_clock_mhz": p.sm_clock_mhz, "sms": p.sms}
+
+
+def write_field(base, data, cells, extensions):
+    """writeToFile's stochastic part: `data` (numpy array or CUDA tensor, float64 or float32,
+    dimension 0 fastest) to <base>.stoch.h5 (dataset /stochastic, F64LE) and <base>.xdmf."""
+    dim = len(cells)
+    ptr, mem = _ptr(data)
+    prec = PREC_F64 if str(getattr(data, "dtype", "")).endswith("float64") else PREC_F32
+    _check(lib().pf_field_write(str(base).encode(), dim, (C.c_int32 * dim)(*cells),
+                                (C.c_double * dim)(*extensions), ptr, prec, mem))
+
+
+def read_field(base, cells, out=None, precision=PREC_F64):
+    """StochasticPart(traits, fileName): <base>.stoch.h5 into `out` (numpy array or CUDA
+    tensor; a new float64 / float32 numpy array when None)."""
+    dim = len(cells)
+    n = int(np.prod(cells))
+    if out is None:
+        out = np.empty(n, dtype=np.float64 if precision == PREC_F64 else np.float32)
+    else:
+        precision = PREC_F64 if str(getattr(out, "dtype", "")).endswith("float64") else PREC_F32
+    ptr, mem = _ptr(out)
+    _check(lib().pf_field_read(str(base).encode(), dim, (C.c_int32 * dim)(*cells), ptr, precision, mem))
+    return out

@@ -4,6 +4,8 @@
 //                                            writing noise, fields and products as raw doubles
 //   facade_main refine <ini> <seed> <outdir> refine / coarsen, without and with a cached
 //                                            inverse product (randomField.cacheInvMatvec)
+//   facade_main io <ini> <seed> <outdir>     writeToFile, then RandomField(fileName) and
+//                                            RandomField(config, fileName) read it back
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -43,6 +45,23 @@ static int run(const ParameterTree& cfg, unsigned seed, const std::string& out) 
   dump(out + "/cinvcx.bin", field.dataVector());
   field.generateUncorrelated(seed);
   dump(out + "/white.bin", field.dataVector());
+  return 0;
+}
+
+template <unsigned dim>
+static int io_run(const ParameterTree& cfg, unsigned seed, const std::string& out) {
+  RandomField<dim> field(cfg);
+  field.generate(seed);
+  field.writeToFile(out + "/saved");
+  RandomField<dim> again(out + "/saved");
+  RandomField<dim> again2(cfg, out + "/saved");
+  if (again.dataVector() != field.dataVector() || again2.dataVector() != field.dataVector()) return 3;
+  // the product of the read field equals the product of the original
+  field.timesMatrix();
+  again.timesMatrix();
+  dump(out + "/a.bin", field.dataVector());
+  dump(out + "/b.bin", again.dataVector());
+  std::printf("io ok\n");
   return 0;
 }
 
@@ -102,6 +121,8 @@ int main(int argc, char** argv) {
     }
     const unsigned seed = (unsigned)std::stoul(argv[3]);
     if (mode == "refine") return dim == 2 ? refine_run<2>(cfg, seed, argv[4]) : refine_run<3>(cfg, seed, argv[4]);
+    if (mode == "io")
+      return dim == 1 ? io_run<1>(cfg, seed, argv[4]) : (dim == 2 ? io_run<2>(cfg, seed, argv[4]) : io_run<3>(cfg, seed, argv[4]));
     if (dim == 1) return run<1>(cfg, seed, argv[4]);
     if (dim == 2) return run<2>(cfg, seed, argv[4]);
     return run<3>(cfg, seed, argv[4]);

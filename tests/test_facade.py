@@ -137,3 +137,21 @@ def test_facade_refine_coarsen(facade_exe, tmp_path, oracle):
     lam, _, _ = oracle.spectrum(d_fine)
     ref = 4.0 * oracle.matvec(d_fine, lam, pfb200.OP_MUL, fine.ravel())
     assert rel(ld("cached_refined.bin"), ref) < 1e-12
+
+
+@pytest.mark.gpu
+def test_facade_write_and_read_field_files(facade_exe, tmp_path):
+    """writeToFile (randomfield.hh:706-713) writes <name>.stoch.h5, <name>.xdmf and <name>.field;
+    RandomField(fileName) and RandomField(config, fileName) read the same field back."""
+    ini = write_ini(tmp_path, "grid.cells = 24 20 12\ngrid.extensions = 1 1 0.5\nstochastic.variance = 1\n"
+                    "stochastic.covariance = exponential\nstochastic.corrLength = 0.1\n")
+    r = subprocess.run([facade_exe, "io", ini, "9", str(tmp_path)], capture_output=True, text=True)
+    assert r.returncode == 0 and "io ok" in r.stdout, r.stdout + r.stderr
+    for ext in (".stoch.h5", ".xdmf", ".field"):
+        assert (tmp_path / ("saved" + ext)).exists()
+    assert '[ grid ]\ncells = "24 20 12"' in (tmp_path / "saved.field").read_text()
+    a = np.fromfile(str(tmp_path / "a.bin"), dtype=np.float64)
+    b = np.fromfile(str(tmp_path / "b.bin"), dtype=np.float64)
+    assert np.array_equal(a, b)
+    field = pfb200.read_field(tmp_path / "saved", (24, 20, 12))
+    assert field.size == 24 * 20 * 12 and np.isfinite(field).all()
