@@ -472,11 +472,18 @@ static pf_status run_pass(pf_plan* P, const char* name, int L, int Lout, long lo
   a.sign2 = sign2;
   TRY(schedule<T>(P, L, &a));
   tile_params(L, (int)sizeof(cx<T>), CONTIG, &a);
-  if (a.blue.M) a.B = 1;
+  if (a.blue.M) {
+    // Bluestein: one row per tile, or up to 8 interleaved strided pencils (coalesced row
+    // segments) while two CTAs still fit on an SM
+    a.B = 1;
+    if (!CONTIG)
+      while (a.B < 8 && (size_t)2 * a.B * (L + a.blue.M) * sizeof(cx<T>) <= 110 * 1024) a.B *= 2;
+  }
   const cx<T>* tw = nullptr;
   TRY(twiddles<T>(P, L, &tw));
-  // Bluestein: the tile buffer plus the M-element scratch in place of the second buffer
-  const size_t smem = a.blue.M ? ((size_t)(CONTIG ? a.pitch : L) + a.blue.M) * sizeof(cx<T>)
+  // Bluestein: the tile buffer plus the M-element scratch (per pencil) in place of the
+  // second buffer
+  const size_t smem = a.blue.M ? ((size_t)(CONTIG ? a.pitch : L) + a.blue.M) * a.B * sizeof(cx<T>)
                                : smem_of(a, CONTIG, (int)sizeof(cx<T>));
   if (smem > 227 * 1024) return fail(PF_ERR_CONFIG, "pencil of length %d does not fit in shared memory", L);
   auto kern = k_pass<T, CONTIG, Ld, Mid, St>;

@@ -276,81 +276,99 @@ __device__ __forceinline__ cx<T> cj_if(cx<T> v, bool c) {
   return v;
 }
 
-// in place on x[0..L) (unit stride); work holds M elements of shared memory
+// in place on the B = 2^lgB pencils of x, element j of pencil b at x[j*B + b] (j < L);
+// work holds M*B elements of shared memory in the same interleaved layout.  M, the
+// butterfly spans and the pencil count are powers of two, so every index is a shift/mask.
 template <typename T>
-__device__ void bluestein(cx<T>* x, cx<T>* work, int L, const Blue& bl, int sign) {
+__device__ void bluestein(cx<T>* x, cx<T>* work, int L, const Blue& bl, int sign, int lgB = 0) {
   const int M = bl.M;
+  const int B = 1 << lgB, bm = B - 1;
+  const int lgM = __ffs(M) - 1;
   const cx<T>* chirp = (const cx<T>*)bl.chirp;
   const cx<T>* bhat = (const cx<T>*)bl.bhat;
   const cx<T>* twM = (const cx<T>*)bl.twM;
   const bool c = sign > 0;
-  for (int u = threadIdx.x; u < M; u += blockDim.x)
-    work[u] = u < L ? cmul<T>(x[u], cj_if<T>(__ldg(chirp + u), c)) : mk<T>(0, 0);
+  for (int u = threadIdx.x; u < (M << lgB); u += blockDim.x) {
+    const int j = u >> lgB;
+    work[u] = j < L ? cmul<T>(x[u], cj_if<T>(__ldg(chirp + j), c)) : mk<T>(0, 0);
+  }
   __syncthreads();
   // forward DIF, natural -> bit-reversed; two radix-2 stages (half H, H/2) per pass over
   // shared memory, a last single stage when log2 M is odd
-  int half = M >> 1;
-  for (; half >= 2; half >>= 2) {
-    const int q = half >> 1;
-    for (int u = threadIdx.x; u < (M >> 2); u += blockDim.x) {
-      const int g = u / q, pos = u - g * q;
+  int half = M >> 1, lgh = lgM - 1;
+  for (; half >= 2; half >>= 2, lgh -= 2) {
+    const int q = half >> 1, lgq = lgh - 1;
+    const int lts = lgM - 1 - lgh;  // log2(M / (2 half))
+    for (int u = threadIdx.x; u < ((M >> 2) << lgB); u += blockDim.x) {
+      const int b = u & bm, v = u >> lgB;
+      const int g = v >> lgq, pos = v & (q - 1);
       const int i0 = g * 2 * half + pos;
-      cx<T> a0 = work[i0], a1 = work[i0 + q], a2 = work[i0 + half], a3 = work[i0 + half + q];
-      const int ts = M / (2 * half);
-      const cx<T> wA0 = __ldg(twM + pos * ts), wA1 = __ldg(twM + (pos + q) * ts), wB = __ldg(twM + pos * 2 * ts);
+      cx<T>* w0 = work + ((size_t)i0 << lgB) + b;
+      const size_t sq = (size_t)q << lgB, sh = (size_t)half << lgB;
+      cx<T> a0 = w0[0], a1 = w0[sq], a2 = w0[sh], a3 = w0[sh + sq];
+      const cx<T> wA0 = __ldg(twM + (pos << lts)), wA1 = __ldg(twM + ((pos + q) << lts)),
+                  wB = __ldg(twM + (pos << (lts + 1)));
       cx<T> s0 = cadd<T>(a0, a2), d0 = cmul<T>(csub<T>(a0, a2), wA0);
       cx<T> s1 = cadd<T>(a1, a3), d1 = cmul<T>(csub<T>(a1, a3), wA1);
-      work[i0] = cadd<T>(s0, s1);
-      work[i0 + q] = cmul<T>(csub<T>(s0, s1), wB);
-      work[i0 + half] = cadd<T>(d0, d1);
-      work[i0 + half + q] = cmul<T>(csub<T>(d0, d1), wB);
+      w0[0] = cadd<T>(s0, s1);
+      w0[sq] = cmul<T>(csub<T>(s0, s1), wB);
+      w0[sh] = cadd<T>(d0, d1);
+      w0[sh + sq] = cmul<T>(csub<T>(d0, d1), wB);
     }
     __syncthreads();
   }
   if (half == 1) {
-    for (int u = threadIdx.x; u < (M >> 1); u += blockDim.x) {
-      const cx<T> a = work[2 * u], b = work[2 * u + 1];
-      work[2 * u] = cadd<T>(a, b);
-      work[2 * u + 1] = csub<T>(a, b);
+    for (int u = threadIdx.x; u < ((M >> 1) << lgB); u += blockDim.x) {
+      const int b = u & bm, v = u >> lgB;
+      cx<T>* w0 = work + ((size_t)(2 * v) << lgB) + b;
+      const cx<T> a = w0[0], bb = w0[B];
+      w0[0] = cadd<T>(a, bb);
+      w0[B] = csub<T>(a, bb);
     }
     __syncthreads();
   }
-  for (int u = threadIdx.x; u < M; u += blockDim.x) work[u] = cmul<T>(work[u], cj_if<T>(__ldg(bhat + u), c));
+  for (int u = threadIdx.x; u < (M << lgB); u += blockDim.x)
+    work[u] = cmul<T>(work[u], cj_if<T>(__ldg(bhat + (u >> lgB)), c));
   __syncthreads();
   // inverse DIT, bit-reversed -> natural; radix-2 stage first when log2 M is odd, then
   // pairs of stages (half h, 2h)
-  int h = 1;
-  int lg = 0;
-  while ((1 << lg) < M) lg++;
-  if (lg & 1) {
-    for (int u = threadIdx.x; u < (M >> 1); u += blockDim.x) {
-      const cx<T> a = work[2 * u], b = work[2 * u + 1];
-      work[2 * u] = cadd<T>(a, b);
-      work[2 * u + 1] = csub<T>(a, b);
+  int h = 1, lgh2 = 0;
+  if (lgM & 1) {
+    for (int u = threadIdx.x; u < ((M >> 1) << lgB); u += blockDim.x) {
+      const int b = u & bm, v = u >> lgB;
+      cx<T>* w0 = work + ((size_t)(2 * v) << lgB) + b;
+      const cx<T> a = w0[0], bb = w0[B];
+      w0[0] = cadd<T>(a, bb);
+      w0[B] = csub<T>(a, bb);
     }
     __syncthreads();
     h = 2;
+    lgh2 = 1;
   }
-  for (; h < M; h <<= 2) {
-    for (int u = threadIdx.x; u < (M >> 2); u += blockDim.x) {
-      const int g = u / h, pos = u - g * h;
+  for (; h < M; h <<= 2, lgh2 += 2) {
+    const int ltA = lgM - 1 - lgh2, ltB = lgM - 2 - lgh2;  // log2(M / 2h), log2(M / 4h)
+    for (int u = threadIdx.x; u < ((M >> 2) << lgB); u += blockDim.x) {
+      const int b = u & bm, v = u >> lgB;
+      const int g = v >> lgh2, pos = v & (h - 1);
       const int i0 = g * 4 * h + pos;
-      const int tsA = M / (2 * h), tsB = M / (4 * h);
-      const cx<T> wA = conjg<T>(__ldg(twM + pos * tsA));
-      const cx<T> wB0 = conjg<T>(__ldg(twM + pos * tsB)), wB1 = conjg<T>(__ldg(twM + (pos + h) * tsB));
-      const cx<T> a0 = work[i0], a1 = cmul<T>(work[i0 + h], wA);
-      const cx<T> a2 = work[i0 + 2 * h], a3 = cmul<T>(work[i0 + 3 * h], wA);
+      cx<T>* w0 = work + ((size_t)i0 << lgB) + b;
+      const size_t s1h = (size_t)h << lgB;
+      const cx<T> wA = conjg<T>(__ldg(twM + (pos << ltA)));
+      const cx<T> wB0 = conjg<T>(__ldg(twM + (pos << ltB))), wB1 = conjg<T>(__ldg(twM + ((pos + h) << ltB)));
+      const cx<T> a0 = w0[0], a1 = cmul<T>(w0[s1h], wA);
+      const cx<T> a2 = w0[2 * s1h], a3 = cmul<T>(w0[3 * s1h], wA);
       const cx<T> s0 = cadd<T>(a0, a1), d0 = csub<T>(a0, a1);
       const cx<T> s1 = cadd<T>(a2, a3), d1 = csub<T>(a2, a3);
       const cx<T> t0 = cmul<T>(s1, wB0), t1 = cmul<T>(d1, wB1);
-      work[i0] = cadd<T>(s0, t0);
-      work[i0 + 2 * h] = csub<T>(s0, t0);
-      work[i0 + h] = cadd<T>(d0, t1);
-      work[i0 + 3 * h] = csub<T>(d0, t1);
+      w0[0] = cadd<T>(s0, t0);
+      w0[2 * s1h] = csub<T>(s0, t0);
+      w0[s1h] = cadd<T>(d0, t1);
+      w0[3 * s1h] = csub<T>(d0, t1);
     }
     __syncthreads();
   }
-  for (int k = threadIdx.x; k < L; k += blockDim.x) x[k] = cmul<T>(work[k], cj_if<T>(__ldg(chirp + k), c));
+  for (int u = threadIdx.x; u < (L << lgB); u += blockDim.x)
+    x[u] = cmul<T>(work[u], cj_if<T>(__ldg(chirp + (u >> lgB)), c));
   __syncthreads();
 }
 

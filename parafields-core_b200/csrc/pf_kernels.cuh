@@ -48,8 +48,8 @@ struct PassArgs {
 template <typename T>
 __device__ __forceinline__ cx<T>* fft_any(cx<T>* b0, cx<T>* b1, cx<T>* work, const TileShape& ts, const PassArgs& a,
                                           const cx<T>* __restrict__ tw, int sign) {
-  if (a.blue.M) {
-    bluestein<T>(b0, work, a.L, a.blue, sign);
+  if (a.blue.M) {  // strided tiles hold B = 2^k interleaved pencils, row tiles one
+    bluestein<T>(b0, work, a.L, a.blue, sign, ts.bfast ? __ffs(ts.B) - 1 : 0);
     return b0;
   }
   return fft_tile<T>(b0, b1, ts, a.rad, tw, sign);
