@@ -63,12 +63,20 @@ struct NoMid {
   }
 };
 
+// loaders that produce elements j and j + L/2 of a pencil from one generator call
+struct R2CNoise;
+template <class Ld>
+struct has_pair_load : std::false_type {};
+template <>
+struct has_pair_load<R2CNoise> : std::true_type {};
+
 // Generic complex pencil pass.  CONTIG: pencils are rows (element j of row p at
 // stride 1); otherwise pencil p of outer block o has element j at p + j*jstride +
 // o*ostride, and one tile holds B consecutive p so every row segment is coalesced.
+// Registers are capped for two resident CTAs per SM (the Bluestein tiles allow two).
 template <typename T, bool CONTIG, class Ld, class Mid, class St>
-__global__ void __launch_bounds__(kThreads) k_pass(const PassArgs a, const cx<T>* __restrict__ tw,
-                                                   Ld ld, Mid mid, St st) {
+__global__ void __launch_bounds__(kThreads, 2) k_pass(const PassArgs a, const cx<T>* __restrict__ tw,
+                                                      Ld ld, Mid mid, St st) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
   TileShape ts;
@@ -94,18 +102,41 @@ __global__ void __launch_bounds__(kThreads) k_pass(const PassArgs a, const cx<T>
     p0 = (blockIdx.x - io * tpo) * a.B;
   }
   const int tot = a.B * a.L;
-  for (int u = threadIdx.x; u < tot; u += blockDim.x) {
-    int b, j;
-    if (CONTIG) {
-      b = u / a.L;
-      j = u - b * a.L;
-    } else {
-      b = u % a.B;
-      j = u / a.B;
+  bool loaded = false;
+  if constexpr (has_pair_load<Ld>::value) {
+    if (a.L % 2 == 0) {  // one generator call for elements j and j + L/2
+      const int h = a.L / 2;
+      for (int u = threadIdx.x; u < a.B * h; u += blockDim.x) {
+        int b, j;
+        if (CONTIG) {
+          b = u / h;
+          j = u - b * h;
+        } else {
+          b = u % a.B;
+          j = u / a.B;
+        }
+        const long long p = p0 + b;
+        cx<T> v0 = mk<T>(0, 0), v1 = mk<T>(0, 0);
+        if (p < a.npencil) ld.template load2<T>((int)p, j, (int)io, v0, v1);
+        b0[b * ts.sb + j * ts.sj] = v0;
+        b0[b * ts.sb + (j + h) * ts.sj] = v1;
+      }
+      loaded = true;
     }
-    const long long p = p0 + b;
-    b0[b * ts.sb + j * ts.sj] = (p < a.npencil) ? ld.template load<T>(p, j, io) : mk<T>(0, 0);
   }
+  if (!loaded)
+    for (int u = threadIdx.x; u < tot; u += blockDim.x) {
+      int b, j;
+      if (CONTIG) {
+        b = u / a.L;
+        j = u - b * a.L;
+      } else {
+        b = u % a.B;
+        j = u / a.B;
+      }
+      const long long p = p0 + b;
+      b0[b * ts.sb + j * ts.sj] = (p < a.npencil) ? ld.template load<T>(p, j, io) : mk<T>(0, 0);
+    }
   __syncthreads();
   cx<T>* wk = b1;  // Bluestein scratch (b1 is not used as a Stockham buffer then)
   cx<T>* r = fft_any<T>(b0, b1, wk, ts, a, tw, a.sign);
@@ -145,8 +176,8 @@ __global__ void __launch_bounds__(kThreads) k_pass(const PassArgs a, const cx<T>
 // X_k = (Z_k + conj Z_{L-k})/2 - i/2 e^{-2 pi i k/2L} (Z_k - conj Z_{L-k}).
 // twT holds exp(-2 pi i m / 2L).
 template <typename T, class Ld, class St>
-__global__ void __launch_bounds__(kThreads) k_r2c(const PassArgs a, const cx<T>* __restrict__ tw,
-                                                  const cx<T>* __restrict__ twT, Ld ld, St st) {
+__global__ void __launch_bounds__(kThreads, 2) k_r2c(const PassArgs a, const cx<T>* __restrict__ tw,
+                                                     const cx<T>* __restrict__ twT, Ld ld, St st) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
   cx<T>* b1 = b0 + a.B * a.pitch;
@@ -187,8 +218,8 @@ __global__ void __launch_bounds__(kThreads) k_r2c(const PassArgs a, const cx<T>*
 // the DC and Nyquist entries ignored): Z_k = (X_k + conj X_{L-k}) + i e^{+2 pi i k/2L}
 // (X_k - conj X_{L-k}), z = IDFT_L(Z), out_{2m} = Re z_m, out_{2m+1} = Im z_m.
 template <typename T, class Ld, class St>
-__global__ void __launch_bounds__(kThreads) k_c2r(const PassArgs a, const cx<T>* __restrict__ tw,
-                                                  const cx<T>* __restrict__ twT, Ld ld, St st) {
+__global__ void __launch_bounds__(kThreads, 2) k_c2r(const PassArgs a, const cx<T>* __restrict__ tw,
+                                                     const cx<T>* __restrict__ twT, Ld ld, St st) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
   cx<T>* b1 = b0 + a.B * a.pitch;
