@@ -157,11 +157,14 @@ __device__ __forceinline__ void p2_stages(P2 (&v)[8], float4* buf, const float4*
   constexpr int NBF = L / R;
   constexpr bool LAST = Ns * R == L;
   __syncthreads();
+  // TP, NBF and Ns are multiples of 8, so slot(j + 8m) = slot(j) + 9m: one runtime slot
+  // per thread, the rest compile-time offsets
+  static_assert(G::TP % 8 == 0 && NBF % 8 == 0 && Ns % 8 == 0, "slot offsets need multiples of 8");
+  const float4* rd = buf + p2_slot(G::PLQ, q, u);
 #pragma unroll
   for (int i = 0; i < NB; i++) {
-    const int t = u + i * G::TP;
 #pragma unroll
-    for (int r = 0; r < R; r++) v[i * R + r] = p2_of(buf[p2_slot(G::PLQ, q, t + r * NBF)]);
+    for (int r = 0; r < R; r++) v[i * R + r] = p2_of(rd[(i * G::TP + r * NBF) / 8 * 9]);
   }
   __syncthreads();
 #pragma unroll
@@ -175,9 +178,9 @@ __device__ __forceinline__ void p2_stages(P2 (&v)[8], float4* buf, const float4*
 #pragma unroll
       for (int r = 0; r < R; r++) out(t + r * Ns, v[i * R + r]);
     } else {
-      const int base = (t / Ns) * Ns * R + k;
+      float4* wr = buf + p2_slot(G::PLQ, q, (t / Ns) * Ns * R + k);
 #pragma unroll
-      for (int r = 0; r < R; r++) buf[p2_slot(G::PLQ, q, base + r * Ns)] = slot_of(v[i * R + r]);
+      for (int r = 0; r < R; r++) wr[r * Ns / 8 * 9] = slot_of(v[i * R + r]);
     }
   }
   if constexpr (!LAST) p2_stages<L, S, Ns * R, TWOFF + (R - 1) * Ns>(v, buf, tw, u, q, out);
@@ -189,8 +192,9 @@ __device__ __forceinline__ void p2_transform(P2 (&v)[8], float4* buf, const floa
                                              const Out& out) {
   using G = P2Geom<L>;
   pdft8<S>(v);
+  float4* wr = buf + p2_slot(G::PLQ, q, u * 8);  // u*8 + r stays within one group of 8
 #pragma unroll
-  for (int r = 0; r < 8; r++) buf[p2_slot(G::PLQ, q, u * 8 + r)] = slot_of(v[r]);
+  for (int r = 0; r < 8; r++) wr[r] = slot_of(v[r]);
   p2_stages<L, S, 8, 0>(v, buf, tw, u, q, out);
 }
 
@@ -318,6 +322,24 @@ __device__ __forceinline__ float2 box_muller_fast(uint32_t a, uint32_t b) {
   return make_float2(rad * c, rad * s);
 }
 
+// MUFU approximations without the denormal-input handling of the intrinsics; every
+// argument below is a normal number (u1 >= 2^-33, x >= 1e-30, |angle| <= pi and not tiny
+// unless zero), so the results equal __log2f / rsqrtf / __sinf / __cosf
+__device__ __forceinline__ float lg2_ftz(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ void sincos_ftz(float x, float* s, float* c) {
+  asm("sin.approx.ftz.f32 %0, %1;" : "=f"(*s) : "f"(x));
+  asm("cos.approx.ftz.f32 %0, %1;" : "=f"(*c) : "f"(x));
+}
+
 // Box-Muller for pencils A and B at once: (a, b) of pencil A and (c, d) of pencil B give
 // the normal pairs (re, im) of both in the pair layout re = (Re A, Re B), im = (Im A, Im B);
 // the same operations and rounding as box_muller_fast, the products issued as FMUL2/FFMA2
@@ -325,17 +347,17 @@ __device__ __forceinline__ P2 box_muller_pair(uint32_t a, uint32_t b, uint32_t c
   const float2 u1 = f2fma(make_float2(__uint2float_rn(a), __uint2float_rn(c)),
                           make_float2(2.3283064365386963e-10f, 2.3283064365386963e-10f),
                           make_float2(1.1641532182693481e-10f, 1.1641532182693481e-10f));
-  const float2 x2 = f2mul(make_float2(__log2f(u1.x), __log2f(u1.y)),
+  const float2 x2 = f2mul(make_float2(lg2_ftz(u1.x), lg2_ftz(u1.y)),
                           make_float2(-1.3862943611198906f, -1.3862943611198906f));
   const float2 x = make_float2(fmaxf(x2.x, 1e-30f), fmaxf(x2.y, 1e-30f));
-  const float2 rad = f2mul(x, make_float2(rsqrtf(x.x), rsqrtf(x.y)));
+  const float2 rad = f2mul(x, make_float2(rsqrt_ftz(x.x), rsqrt_ftz(x.y)));
   const float2 u2 = f2add(make_float2(__uint_as_float(0x3f800000u | (b >> 9)), __uint_as_float(0x3f800000u | (d >> 9))),
                           make_float2(-1.0f, -1.0f));
   const float2 ang = f2fma(make_float2(6.283185307179586f, 6.283185307179586f), u2,
                            make_float2(-3.141592653589793f, -3.141592653589793f));
   float sA, cA, sB, cB;
-  __sincosf(ang.x, &sA, &cA);
-  __sincosf(ang.y, &sB, &cB);
+  sincos_ftz(ang.x, &sA, &cA);
+  sincos_ftz(ang.y, &sB, &cB);
   return {f2mul(rad, make_float2(cA, cB)), f2mul(rad, make_float2(sA, sB))};
 }
 
