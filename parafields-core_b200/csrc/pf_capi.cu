@@ -620,7 +620,7 @@ static pf_status launch_fpass(pf_plan* P, const char* name, int Lout, long long 
   return prof_end(P, &rec);
 }
 
-#define PF_FAST_LENGTHS(X) X(64) X(128) X(256) X(512) X(1024) X(2048)
+#define PF_FAST_LENGTHS(X) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024) X(1536) X(2048)
 
 template <typename T, int SIGN, int SIGN2, bool CONTIG, bool PAIR, class Ld, class Mid, class St>
 static pf_status run_fpass(pf_plan* P, const char* name, int L, int Lout, long long npencil, long long nouter, Ld ld,

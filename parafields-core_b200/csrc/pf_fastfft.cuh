@@ -23,10 +23,12 @@ constexpr int pick_radix(int m) {
   return (m % 8 == 0) ? 8 : (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2 : (m % 3 == 0) ? 3 : (m % 5 == 0) ? 5 : (m % 7 == 0) ? 7 : m;
 }
 
-// one radix-8 butterfly column per thread and stage: B = 8 * threads / L
+// one radix-8 butterfly column per thread and stage: B = 8 * threads / L, rounded down to
+// a power of two so that B divides the thread count (lengths with a factor 3)
+constexpr int pow2_floor_c(int x) { return x >= 2 ? 2 * pow2_floor_c(x / 2) : 1; }
 template <typename T, int L>
 constexpr int fast_B() {
-  return (8 * kThreads / L) >= 16 ? 16 : ((8 * kThreads / L) >= 1 ? 8 * kThreads / L : 1);
+  return (8 * kThreads / L) >= 16 ? 16 : ((8 * kThreads / L) >= 1 ? pow2_floor_c(8 * kThreads / L) : 1);
 }
 
 // rows of one padded tile buffer holding `rows` logical rows

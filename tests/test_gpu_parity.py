@@ -47,6 +47,11 @@ CONFIGS = {
                             anisotropy="geometric", approximate=True),
     "3d-exp-iso-notransp-pow2": dict(dim=3, cells=(64, 64, 128), covariance="exponential", corr_length=0.05,
                                      transposed=0),
+    # 3-smooth tori (96, 192, 384, 768): the fast scalar kernels with a radix-3 stage
+    "3d-matern32-3smooth": dict(dim=3, cells=(48, 96, 192), covariance="matern32", corr_length=0.1,
+                                approximate=True),
+    "2d-exp-geo-3smooth": dict(dim=2, cells=(384, 96), covariance="exponential",
+                               corr_length=(0.1, 0.02, -0.02, 0.05), anisotropy="geometric", approximate=True),
     # merge periodization (matrix.hh:652-775): radial branch needs sqrt(dim) < factor/2
     "2d-merge-radialplus-f3": dict(dim=2, cells=(48, 40), covariance="matern32", corr_length=0.3,
                                    embedding_factor=3, periodization="merge", sigmoid_start=1.0,
