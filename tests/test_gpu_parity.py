@@ -52,6 +52,9 @@ CONFIGS = {
                                 approximate=True),
     "2d-exp-geo-3smooth": dict(dim=2, cells=(384, 96), covariance="exponential",
                                corr_length=(0.1, 0.02, -0.02, 0.05), anisotropy="geometric", approximate=True),
+    # 5-smooth tori (160, 320, 640): radix-5 stages of the generic kernels
+    "3d-exp-5smooth": dict(dim=3, cells=(80, 160, 320), covariance="exponential", corr_length=0.08,
+                           approximate=True),
     # merge periodization (matrix.hh:652-775): radial branch needs sqrt(dim) < factor/2
     "2d-merge-radialplus-f3": dict(dim=2, cells=(48, 40), covariance="matern32", corr_length=0.3,
                                    embedding_factor=3, periodization="merge", sigmoid_start=1.0,
