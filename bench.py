@@ -130,6 +130,25 @@ def dist_setup(n):
     return 0, 1, 0
 
 
+def replica_seed(rank):
+    """Base seed of one replica's realizations: every rank generates its own, distinct fields."""
+    return 1000003 * (rank + 1)
+
+
+def max_over_ranks(value, world, device):
+    """The slowest rank's value (every rank takes part in the reduction)."""
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world, units, steps, seconds):
+    """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
+    return world * units * steps / seconds
+
+
 def cpu_oracle_realization(threads):
     """one FP64 realization of the workload with the CPU restatement (spectrum untimed)"""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -196,7 +215,7 @@ def run_b200(args):
     # the K timed realizations go through one pf_generate_batch call, which alternates them
     # over two streams (one realization's noise pass overlaps the other's transform passes)
     outs = torch.empty(max(args.steps, 2) * n, dtype=torch.float32, device=dev)
-    seed0 = 1000003 * (rank + 1)
+    seed0 = replica_seed(rank)
     P.generate_batch(seed=seed0, count=max(args.warmup, 2), out=outs[: max(args.warmup, 2) * n])
     torch.cuda.synchronize()
     if world > 1:
@@ -218,12 +237,10 @@ def run_b200(args):
     torch.cuda.synchronize()
     prof = P.profile_read()
     P.profile(False)
-    t = torch.tensor([ms], device=dev)
     if world > 1:
         torch.distributed.barrier()
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms = float(t.item())
-    value = world * n * args.steps / (ms / 1e3)
+    ms = max_over_ranks(ms, world, dev)
+    value = aggregate_rate(world, n, args.steps, ms / 1e3)
 
     # end to end through the public call with a host result buffer (D2H inside the region):
     # pf_generate_batch into pinned host memory, every realization copied to the host while
@@ -236,10 +253,7 @@ def run_b200(args):
     P.generate_batch(seed=seed0 + 500, count=ke, out=hp)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    te = torch.tensor([dt], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e = world * n * ke / float(te.item())
+    e2e = aggregate_rate(world, n, ke, max_over_ranks(dt, world, dev))
 
     if rank == 0:
         peak, peak_kind = load_peaks()
