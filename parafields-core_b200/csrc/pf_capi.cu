@@ -1292,10 +1292,14 @@ static pf_status matvec_r2c(pf_plan* P, int op, const S* in, S* out) {
     TRY(workspace(P, 2, sizeof(cx<T>) * (size_t)P0 * g.n[1], &X1));
     TRY((run_freal<T, true>(P, "mv_r2c_d0", g.T[0], T0c, g.n[1], fl, arr_store<cx<T>>(P, X1, 1, 0, P0),
                             (double)g.n[1] * (g.n[0] * sizeof(S) + T0c * e))));
-    TRY((run_fpass<T, -1, +1, false, false>(P, "mv_fused_d1", g.T[1], g.n[1], T0c, 1,
-                                            arr_load<cx<T>>(P, X1, P0, 0, 1, g.n[1]), mid,
-                                            arr_store<cx<T>>(P, X1, P0, 0, 1),
-                                            (double)T0c * (2.0 * g.n[1] * e + g.T[1] * lb))));
+    const double bf1 = (double)T0c * (2.0 * g.n[1] * e + g.T[1] * lb);
+    if (std::is_same<T, float>::value && p2_length(g.T[1]) && p2_view_ok(X1, P0, 0, 1))
+      TRY(p2_c2c_mid(P, "mv_fused_d1", g.T[1], g.n[1], T0c, 1, p2_load(P, X1, P0, 0, g.n[1], T0c), mid,
+                     p2_store(P, X1, P0, 0, T0c), bf1));
+    else
+      TRY((run_fpass<T, -1, +1, false, false>(P, "mv_fused_d1", g.T[1], g.n[1], T0c, 1,
+                                              arr_load<cx<T>>(P, X1, P0, 0, 1, g.n[1]), mid,
+                                              arr_store<cx<T>>(P, X1, P0, 0, 1), bf1)));
     return run_freal<T, false>(P, "mv_c2r_d0", g.T[0], g.n[0], g.n[1], arr_load<cx<T>>(P, X1, 1, 0, P0, T0c), fs,
                                (double)g.n[1] * (T0c * e + g.n[0] * sizeof(S)));
   }
@@ -1311,10 +1315,14 @@ static pf_status matvec_r2c(pf_plan* P, int op, const S* in, S* out) {
                                           arr_store<cx<T>>(P, X2, P0, s2, 1),
                                           (double)T0c * g.n[2] * (g.n[1] + g.T[1]) * e)));
   // forward along dim 2, eigenvalue factor, backward along dim 2 (pencils k0 x k1)
-  TRY((run_fpass<T, -1, +1, false, false>(P, "mv_fused_d2", g.T[2], g.n[2], T0c, g.T[1],
-                                          arr_load<cx<T>>(P, X2, s2, P0, 1, g.n[2]), mid,
-                                          arr_store<cx<T>>(P, X2, s2, P0, 1),
-                                          (double)T0c * g.T[1] * (2.0 * g.n[2] * e + g.T[2] * lb))));
+  const double bf2 = (double)T0c * g.T[1] * (2.0 * g.n[2] * e + g.T[2] * lb);
+  if (std::is_same<T, float>::value && p2_length(g.T[2]) && p2_view_ok(X2, s2, P0, g.T[1]))
+    TRY(p2_c2c_mid(P, "mv_fused_d2", g.T[2], g.n[2], T0c, g.T[1], p2_load(P, X2, s2, P0, g.n[2], T0c), mid,
+                   p2_store(P, X2, s2, P0, T0c), bf2));
+  else
+    TRY((run_fpass<T, -1, +1, false, false>(P, "mv_fused_d2", g.T[2], g.n[2], T0c, g.T[1],
+                                            arr_load<cx<T>>(P, X2, s2, P0, 1, g.n[2]), mid,
+                                            arr_store<cx<T>>(P, X2, s2, P0, 1), bf2)));
   TRY((run_fpass<T, +1, +1, false, false>(P, "mv_c2c_d1i", g.T[1], g.n[1], T0c, g.n[2],
                                           arr_load<cx<T>>(P, X2, P0, s2, 1, g.T[1]), NoMid(),
                                           arr_store<cx<T>>(P, X1, P0, (long long)P0 * g.n[1], 1),

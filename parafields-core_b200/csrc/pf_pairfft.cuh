@@ -592,6 +592,54 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
 }
 
 // ---------------------------------------------------------------------------
+// Fused strided pass of the matvec: forward transform, a per-element operator (Mid, e.g.
+// the eigenvalue factor) and the backward transform of the same pencils, the spectrum
+// staying in shared memory between the two (tables of both directions in shared memory).
+// ---------------------------------------------------------------------------
+template <int L, class Mid>
+__global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
+    kp2_c2c_mid(const float4* __restrict__ twf, const float4* __restrict__ twb, long long ntiles, int tpo,
+                int Lout, P2ArrLoad ld, Mid mid, P2ArrStore st) {
+  using G = P2Geom<L>;
+  extern __shared__ __align__(16) float4 p2_smem[];
+  float4* buf = p2_smem;
+  float4* tf = p2_smem + G::Q * G::PLQ;
+  float4* tb = tf + G::NTW;
+  p2_copy_table(tf, twf, G::NTW);
+  p2_copy_table(tb, twb, G::NTW);
+  __syncthreads();
+  const int q = threadIdx.x % G::Q, u = threadIdx.x / G::Q;
+  unsigned bad = 0;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int o = (int)(tile / tpo);
+    const int p = (int)(tile - (long long)o * tpo) * G::NP + 2 * q;
+    P2 v[8];
+    const P2ArrLoad::Tile lt = ld.tile(p, o, bad);
+#pragma unroll
+    for (int r = 0; r < 8; r++) v[r] = ld.load_t(lt, u + r * G::TP);
+    // forward transform; its outputs land in the exchange buffer (its last stage has read
+    // the buffer and passed a barrier before the first output is written)
+    p2_transform<L, -1>(v, buf, tf, u, q, [&](int j, const P2& x) { buf[p2_slot(G::PLQ, q, j)] = slot_of(x); });
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const int j = u + r * G::TP;
+      const P2 x = p2_of(buf[p2_slot(G::PLQ, q, j)]);
+      cx<float> a = mk<float>(0.f, 0.f), b = a;  // pencils beyond the last one stay zero
+      if (p < ld.np) a = mid.template operator()<float>(p, j, o, mk<float>(x.re.x, x.im.x));
+      if (p + 1 < ld.np) b = mid.template operator()<float>(p + 1, j, o, mk<float>(x.re.y, x.im.y));
+      v[r] = {make_float2(a.x, b.x), make_float2(a.y, b.y)};
+    }
+    __syncthreads();
+    const P2ArrStore::Tile so = st.tile(p, o, Lout, bad);
+    p2_transform<L, +1>(v, buf, tb, u, q, [&](int j, const P2& x) {
+      if (j < Lout) st.store_t(so, j, x);
+    });
+  }
+  p2_report(bad);
+}
+
+// ---------------------------------------------------------------------------
 // Complex-to-real rows (2L reals from L+1 complex, FFTW c2r semantics: Im of the DC
 // and Nyquist inputs ignored), rows p and p+1 per pair, threads along the row.
 // Store(p, m, x0, x1) receives reals 2m and 2m+1 of row p.

@@ -138,7 +138,9 @@ def test_generate_parity(oracle, name, prec):
 @pytest.mark.parametrize("prec", [pfb200.PREC_F64, pfb200.PREC_F32])
 @pytest.mark.parametrize("op", [pfb200.OP_MUL, pfb200.OP_ROOT, pfb200.OP_INVEXT])
 @pytest.mark.parametrize("name", ["2d-exp-iso", "2d-sph-geo", "3d-gexp-iso-notransp", "3d-exp-geo",
-                                  "3d-matern32-axi", "2d-exp-prime", "3d-sph-prime"])
+                                  "3d-matern32-axi", "2d-exp-prime", "3d-sph-prime",
+                                  # power-of-two tori: FP32 takes the paired fused pass
+                                  "2d-exp-pow2", "3d-matern32-axi-pow2", "3d-exp-geo-pow2"])
 def test_matvec_parity(oracle, name, op, prec):
     d, P, lam, st, _ = plan_and_oracle(oracle, CONFIGS[name])
     if op == pfb200.OP_INVEXT and (lam <= 0).any():
