@@ -52,19 +52,30 @@ def realization_work(cells, torus):
     """Compulsory HBM bytes and FFT flops of one FP32 realization with in-register noise
     (per-unit figures of the measurement plan): bytes = sqrt(lambda) on the prod(T/2+1) DCT
     cells (FP32) + the field (FP32); flops = 2.5 N log2 N for the real 3D transform of the
-    torus, N = prod(T).  Also the flops of each pass of the pruned schedule the library runs
-    (complex pencils: 5 L log2 L; the final complex-to-real rows: 2.5 L log2 L)."""
+    torus, N = prod(T).  Also, per pass of the pruned three-pass schedule the library runs,
+    the bytes that pass cannot avoid (each input read once from HBM, each output written
+    once) and its flops (complex pencils: 5 L log2 L; the final complex-to-real rows:
+    2.5 L log2 L):
+      gen_noise_last  sqrt(lambda) on the DCT cells (mirrored reads of a cell are L2 hits)
+                      + the (T0/2+1) T1 n2 complex64 planes it keeps
+      gen_c2c_d1      those planes in + (T0/2+1) n1 n2 complex64 out
+      gen_c2r_d0      that array in + the n0 n1 n2 FP32 field out"""
     import math
     t0, t1, t2 = torus
     n0, n1, n2 = cells
     N = t0 * t1 * t2
-    sq = (t0 // 2 + 1) * (t1 // 2 + 1) * (t2 // 2 + 1) * 4
+    c0 = t0 // 2 + 1
+    sq = c0 * (t1 // 2 + 1) * (t2 // 2 + 1) * 4
     out = n0 * n1 * n2 * 4
+    w1 = c0 * t1 * n2 * 8
+    w2 = c0 * n1 * n2 * 8
     c = lambda L: 5.0 * L * math.log2(L)  # noqa: E731
-    passes = {"gen_noise_last": (t0 // 2 + 1) * t1 * c(t2),   # last axis, every pencil of the half spectrum
-              "gen_c2c_d1": (t0 // 2 + 1) * n2 * c(t1),       # axis 1 on the n2 kept planes
-              "gen_c2r_d0": n1 * n2 * 0.5 * c(t0)}            # complex-to-real rows of the kept cells
-    return {"compulsory_bytes": sq + out, "flops": 2.5 * N * math.log2(N), "pass_flops": passes}
+    passes = {"gen_noise_last": c0 * t1 * c(t2),   # last axis, every pencil of the half spectrum
+              "gen_c2c_d1": c0 * n2 * c(t1),       # axis 1 on the n2 kept planes
+              "gen_c2r_d0": n1 * n2 * 0.5 * c(t0)}  # complex-to-real rows of the kept cells
+    pass_bytes = {"gen_noise_last": sq + w1, "gen_c2c_d1": w1 + w2, "gen_c2r_d0": w2 + out}
+    return {"compulsory_bytes": sq + out, "flops": 2.5 * N * math.log2(N), "pass_flops": passes,
+            "pass_bytes": pass_bytes, "schedule_bytes": sum(pass_bytes.values())}
 
 
 def ncu_traffic():
@@ -150,7 +161,9 @@ def aggregate_rate(world, units, steps, seconds):
 
 
 def cpu_oracle_realization(threads):
-    """one FP64 realization of the workload with the CPU restatement (spectrum untimed)"""
+    """One FP64 realization of the workload with the CPU restatement (spectrum and noise
+    untimed).  Returns its time, the cell count, the noise buffer (reference draw order)
+    and the field, so the same noise can be fed to the GPU and the result checked."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     import pfb200
@@ -158,10 +171,38 @@ def cpu_oracle_realization(threads):
     d = pfb200.make_desc(**WORKLOAD)
     g = O.resolve(d)
     lam, _, _ = O.spectrum(d)
-    noise = O.noise(1, g.noise)
+    noise = O.noise(20261203, g.noise)
     t0 = time.perf_counter()
-    O.generate(d, lam, noise)
-    return time.perf_counter() - t0, g.domain
+    field, _ = O.generate(d, lam, noise)
+    return time.perf_counter() - t0, g.domain, noise, field, lam
+
+
+def cpu_scipy_realization(threads, lam, noise, cells=WORKLOAD["cells"]):
+    """The same realization with scipy.fft (pocketfft, `workers` threads) for the transform:
+    eigenvalue-scaled half spectrum (the oracle's noise and eigenvalues, R2C layout with the
+    DCT mirror and the transposed 3D storage order), one irfftn over the torus (2 cells per
+    cell and axis), extraction of the domain.  A library-grade CPU reference point for the
+    transform, timed as the oracle is."""
+    import scipy.fft as sf
+    n = cells
+    t = [2 * c for c in n]
+    c0 = t[0] // 2 + 1
+    D = [x // 2 + 1 for x in t]
+    # DCT layout, dimension 0 fastest, stored dimensions (0, 2, 1) in 3D
+    sq = np.sqrt(lam.reshape(D[1], D[2], D[0])).swapaxes(0, 1)
+    t0 = time.perf_counter()
+    # stored frequency (k0, k1, k2) with the 3D transposed layout: noise pair index
+    # k0 + c0 * (k2 + t2 * k1); eigenvalue at the mirrored DCT cell
+    m1 = np.minimum(np.arange(t[1]), t[1] - np.arange(t[1]))
+    m2 = np.minimum(np.arange(t[2]), t[2] - np.arange(t[2]))
+    z = noise.view(np.complex128).reshape(t[1], t[2], c0).transpose(1, 0, 2)  # (k2, k1, k0)
+    lamc = sq[np.ix_(m2, m1, np.arange(c0))]
+    selfc = np.zeros((t[2], t[1], c0), dtype=bool)
+    selfc[np.ix_([0, t[2] // 2], [0, t[1] // 2], [0, t[0] // 2])] = True
+    spec = np.where(selfc, lamc * z.real, lamc * np.sqrt(0.5) * z)
+    field = sf.irfftn(spec, s=(t[2], t[1], t[0]), workers=threads, norm="forward")[: n[2], : n[1], : n[0]]
+    dt = time.perf_counter() - t0
+    return dt, np.ascontiguousarray(field).ravel()
 
 
 def run_reference(args):
@@ -257,22 +298,30 @@ def run_b200(args):
 
     if rank == 0:
         peak, peak_kind = load_peaks()
+        work = realization_work(WORKLOAD["cells"], CONFIG["torus"])
         dom = max(prof, key=lambda r: r["total_ms"]) if prof else None
         roof = None
         if dom:
             avg_ms = dom["total_ms"] / dom["launches"]
-            bytes_per = dom["bytes"] / dom["launches"]
+            bytes_per = work["pass_bytes"].get(dom["name"], dom["bytes"] / dom["launches"])
             ach = bytes_per / (avg_ms / 1e3) / 1e9
             tr = ncu_traffic().get(dom["name"])
+            sched_gbs = work["schedule_bytes"] / (ms / args.steps / 1e3) / 1e9
             roof = {"kernel": dom["name"], "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
-                    "note": "kernel durations from CUDA events around each launch on the plan's stream, "
-                            "over the same number of realizations generated one at a time after the "
-                            "timed (pipelined) region",
+                    "note": "achieved = the pass's compulsory bytes (each input read once, each output "
+                            "written once) / its mean CUDA-event duration on the plan's stream, over the "
+                            "same number of realizations generated one at a time after the timed "
+                            "(pipelined) region; traffic = ncu DRAM bytes of one launch "
+                            "(profiles/ncu_traffic.txt); the pass is instruction-issue-bound, not "
+                            "DRAM-bound (see compute.dominant_kernel)",
                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach / peak, 4),
                     "traffic": tr, "algorithmic_bytes_per_launch": bytes_per, "avg_launch_ms": avg_ms,
-                    "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()}
+                    "schedule": {"bytes_per_realization": work["schedule_bytes"],
+                                 "gbs": round(sched_gbs, 1), "frac": round(sched_gbs / peak, 4),
+                                 "note": "all three passes' compulsory bytes per realization / ms_per_step"},
+                    "kernels": [dict({k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()},
+                                     compulsory_bytes_per_launch=work["pass_bytes"].get(r["name"]))
                                 for r in prof]}
-        work = realization_work(WORKLOAD["cells"], CONFIG["torus"])
         f32peak = max(fpeaks["fp32_ffma_tflops"], fpeaks["fp32_ffma2_tflops"])
         real_s = ms / args.steps / 1e3
         compute = {
@@ -292,13 +341,31 @@ def run_b200(args):
             tfl = pf / (avg_ms / 1e3) / 1e12
             compute["dominant_kernel"] = {"kernel": dom["name"], "flops": pf, "tflops": round(tfl, 2),
                                           "fp32_frac": round(tfl / f32peak, 4)}
-        cpu = None
+        cpu = cpu_lib = err = None
         if not args.no_cpu_baseline and world == 1:
             threads = os.cpu_count() or 1
-            dt_cpu, cells = cpu_oracle_realization(threads)
+            dt_cpu, cells, noise, ofield, lam = cpu_oracle_realization(threads)
             cpu = {"value": cells / dt_cpu, "unit": "cells/s", "cores": threads, "kind": "port",
                    "sample": "1 FP64 realization of the same workload by the CPU restatement (oracle/), "
                              f"{dt_cpu:.1f} s; spectrum and noise drawn outside the timed region"}
+            dt_lib, sfield = cpu_scipy_realization(threads, lam, noise)
+            cpu_lib = {"value": cells / dt_lib, "unit": "cells/s", "cores": threads, "kind": "library",
+                       "sample": "the same FP64 realization with scipy.fft.irfftn (pocketfft, workers="
+                                 f"{threads}) for the transform, {dt_lib:.1f} s; eigenvalue scaling and "
+                                 "extraction in numpy",
+                       "rel_l2_vs_oracle": float(np.linalg.norm(sfield - ofield) / np.linalg.norm(ofield))}
+            # the FP32 GPU realization from the oracle's noise buffer (reference draw order),
+            # outside the timed region
+            hn = torch.from_numpy(noise).to(dev)
+            P.generate(noise=hn, out=out)
+            torch.cuda.synchronize()
+            gf = out.double().cpu().numpy()
+            err = {"rel_l2_error_vs_oracle": float(np.linalg.norm(gf - ofield) / np.linalg.norm(ofield)),
+                   "max_abs_error_vs_oracle": float(np.abs(gf - ofield).max()),
+                   "note": "one FP32 realization of the timed workload fed the oracle's N(0,1) buffer "
+                           "(seed 20261203, reference draw order), against the FP64 oracle on the same "
+                           "buffer; tolerance of the parity tests 1e-5"}
+            del hn
         clocks = clk.summary()
         line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -309,7 +376,9 @@ def run_b200(args):
                         "note": f"pf_generate_batch(seed, count={ke}, pinned host out): seed passed by value, "
                                 "every realization copied to the host inside the region while the next one is "
                                 "computed (wall clock)"},
+                "rel_l2_error_vs_oracle": err["rel_l2_error_vs_oracle"] if err else None, "error": err,
                 "gpu_launches": launches, "roofline": roof, "compute": compute, "cpu_baseline": cpu,
+                "cpu_baseline_library_fft": cpu_lib,
                 "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"],
                            "reasons": clocks["reasons"]}}
         print(json.dumps(line), flush=True)
@@ -384,7 +453,7 @@ def c3_descs(count, precision, seed=20261203):
 
 def run_ensemble(args):
     """Uneven 2D fields: mixed (FP32 realizations, FP64 spectra) graph replay vs FP64 replay
-    vs the plain FP64 path (one plan and one pf_generate per field)."""
+    vs the plain FP64 path (one plan and one pf_generate per field, every field)."""
     import torch
     import pfb200
     count = args.fields
@@ -396,6 +465,9 @@ def run_ensemble(args):
         st = E.spectra()
         torch.cuda.synchronize()
         tspec = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        timed = E.autotune(repetitions=1) if not args.no_tune else 0
+        ttune = time.perf_counter() - t0
         out = torch.empty(E.total, dtype=torch.float32 if prec else torch.float64, device="cuda")
         E.generate(out)
         s = torch.cuda.current_stream()
@@ -409,12 +481,13 @@ def run_ensemble(args):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
         res[name] = {"cells": E.total, "ms_per_ensemble": ms, "cells_per_s": E.total / (ms / 1e3),
-                     "spectra_s": tspec, "fields_with_negative_eigenvalues": sum(1 for x in st if x["negative"]),
+                     "spectra_s": tspec, "autotune_s": ttune, "fields_timed_by_autotune": timed,
+                     "fields_with_negative_eigenvalues": sum(1 for x in st if x["negative"]),
                      "launches_per_replay": E.launches_per_replay()}
         E.close()
         del out
         torch.cuda.empty_cache()
-    sub = c3_descs(count, pfb200.PREC_F64)[: min(count, 256)]
+    sub = c3_descs(count, pfb200.PREC_F64)
     cells, ms_tot = 0, 0.0
     s = torch.cuda.current_stream()
     for dsc in sub:
@@ -467,22 +540,21 @@ def run_cinv(args):
     loss1 = Lp.train(Bt, Xt, epochs=args.epochs, lr=args.lr, fp32=True)
     ttrain = time.perf_counter() - t0
     Bs = torch.tensor(rng.standard_normal((K_test, N)), device="cuda")
-    x = torch.empty(N, dtype=torch.float64, device="cuda")
+    X = torch.empty_like(Bs)
     out = {}
-    for name, attach in (("plain", False), ("learned", True)):
+    for name, attach, lanes in (("plain", False, args.lanes), ("plain_one_lane", False, 1),
+                                ("learned", True, 1)):
         Lp.attach(attach)
-        it, res = 0, []
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for i in range(K_test):
-            _, rep = P.multiply_inverse(Bs[i], x=x, mode=pfb200.CG_RESIDUAL, tolerance=1e-8, inner_fp32=True,
-                                        max_iterations=20000)
-            it += rep["iterations"]
-            res.append(rep["relative_residual"])
+        _, reps = P.multiply_inverse_batch(Bs, X, lanes=lanes, mode=pfb200.CG_RESIDUAL, tolerance=1e-8,
+                                           inner_fp32=True, max_iterations=20000)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
+        it = sum(r["iterations"] for r in reps)
         out[name] = {"solves_per_s": K_test / dt, "s_per_solve": dt / K_test, "iterations_per_solve": it / K_test,
-                     "max_relative_residual": max(res)}
+                     "max_relative_residual": max(r["relative_residual"] for r in reps), "lanes": lanes,
+                     "s_per_iteration": dt / max(it, 1) * min(lanes, K_test)}
     Lp.attach(False)
     print(json.dumps({"metric": f"C^-1 solves/s ({n}^3 exponential, geometric anisotropy, 1e-8 FP64 residual)",
                       "unit": "solves/s", "value": out["plain"]["solves_per_s"], "dtype": "f32 inner / f64 residual",
@@ -537,6 +609,8 @@ def main():
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--residual-loss", action="store_true")
     ap.add_argument("--lr", type=float, default=0.005)
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--lanes", type=int, default=4)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

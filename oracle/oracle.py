@@ -131,8 +131,25 @@ def dct1(x):
 
 
 def covariance(desc, x):
+    """c at the already transformed distance vector x (covariance.hh:296-823)"""
     x = np.ascontiguousarray(x, dtype=np.float64)
     return lib().oc_covariance(C.byref(desc), _dp(x))
+
+
+def geometry(desc, x):
+    """the anisotropy transform of a physical distance vector (covariance.hh:18-138)"""
+    v = np.zeros(3)
+    x = np.asarray(x, dtype=np.float64).ravel()
+    v[: x.size] = x
+    x = v
+    out = np.zeros(3)
+    lib().oc_geometry(C.byref(desc), _dp(np.ascontiguousarray(x)), _dp(out))
+    return out
+
+
+def prescribed_covariance(desc, lag):
+    """c(h) of the configured covariance at the physical lag vector h"""
+    return covariance(desc, geometry(desc, lag))
 
 
 def fill_matrix(desc):

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import pfb200
-from helpers import desc_of, rel
+from helpers import counter_noise, desc_of, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -81,6 +81,22 @@ CONFIGS = {
     "2d-cofold-geo-r2c-f4": dict(dim=2, cells=(24, 20), covariance="exponential",
                                  corr_length=(0.4, 0.1, -0.1, 0.3), anisotropy="geometric", embedding_factor=4,
                                  periodization="cofold", cofold_recursions=3, approximate=True),
+    # the remaining covariance functors (covariance.hh:465-489, 633-744, 799-823)
+    "2d-sepexp-axi": dict(dim=2, cells=(48, 40), covariance="separableExponential", corr_length=(0.1, 0.2),
+                          anisotropy="axiparallel"),
+    "3d-sepexp-iso": dict(dim=3, cells=(16, 20, 12), covariance="separableExponential", corr_length=0.1),
+    "2d-damped-iso": dict(dim=2, cells=(48, 40), covariance="dampedOscillation", corr_length=0.1),
+    "3d-damped-geo": dict(dim=3, cells=(16, 12, 12), covariance="dampedOscillation",
+                          corr_length=(0.1, 0.02, 0.0, -0.02, 0.08, 0.0, 0.0, 0.0, 0.05), anisotropy="geometric"),
+    "2d-cauchy-geo": dict(dim=2, cells=(40, 32), covariance="cauchy", corr_length=(0.1, 0.02, -0.01, 0.06),
+                          anisotropy="geometric"),
+    "3d-cauchy-iso": dict(dim=3, cells=(16, 16, 12), covariance="cauchy", corr_length=0.08),
+    "2d-gcauchy-axi": dict(dim=2, cells=(40, 48), covariance="generalizedCauchy", cauchy_alpha=1.5, cauchy_beta=0.8,
+                           corr_length=(0.1, 0.05), anisotropy="axiparallel", approximate=True),
+    "3d-gcauchy-iso": dict(dim=3, cells=(12, 16, 20), covariance="generalizedCauchy", cauchy_alpha=0.7,
+                           cauchy_beta=2.5, corr_length=0.1),
+    "2d-white-iso": dict(dim=2, cells=(40, 36), covariance="whiteNoise", corr_length=0.1),
+    "3d-white-iso": dict(dim=3, cells=(12, 10, 8), covariance="whiteNoise", corr_length=0.1),
     # tori whose lengths have prime factors above 13: Bluestein transforms
     "2d-exp-prime": dict(dim=2, cells=(131, 97), covariance="exponential", corr_length=0.1),
     "3d-sph-prime": dict(dim=3, cells=(17, 19, 23), covariance="spherical", corr_length=0.2),
@@ -139,6 +155,8 @@ def test_generate_parity(oracle, name, prec):
 @pytest.mark.parametrize("op", [pfb200.OP_MUL, pfb200.OP_ROOT, pfb200.OP_INVEXT])
 @pytest.mark.parametrize("name", ["2d-exp-iso", "2d-sph-geo", "3d-gexp-iso-notransp", "3d-exp-geo",
                                   "3d-matern32-axi", "2d-exp-prime", "3d-sph-prime",
+                                  "2d-sepexp-axi", "3d-damped-geo", "2d-cauchy-geo", "3d-gcauchy-iso",
+                                  "2d-white-iso",
                                   # power-of-two tori: FP32 takes the paired fused pass
                                   "2d-exp-pow2", "3d-matern32-axi-pow2", "3d-exp-geo-pow2"])
 def test_matvec_parity(oracle, name, op, prec):
@@ -297,63 +315,6 @@ def test_counter_based_noise_statistics(oracle):
     assert (np.abs(emp - exact) < 5 * se + 1e-12).mean() > 0.995
 
 
-# ---------------------------------------------------------------------------
-# counter-based noise, reproduced on the host
-# ---------------------------------------------------------------------------
-def _philox4x32_10(c, seed):
-    """Philox4x32-10 (Salmon et al., SC 2011) on uint64 arrays holding 32-bit words."""
-    m32 = np.uint64(0xFFFFFFFF)
-    c0, c1, c2, c3 = (np.asarray(x, dtype=np.uint64) & m32 for x in c)
-    k0, k1 = np.uint64(seed & 0xFFFFFFFF), np.uint64((seed >> 32) & 0xFFFFFFFF)
-    for _ in range(10):
-        p0 = np.uint64(0xD2511F53) * c0
-        p1 = np.uint64(0xCD9E8D57) * c2
-        c0, c1, c2, c3 = ((p1 >> np.uint64(32)) ^ c1 ^ k0, p1 & m32, (p0 >> np.uint64(32)) ^ c3 ^ k1, p0 & m32)
-        k0 = (k0 + np.uint64(0x9E3779B9)) & m32
-        k1 = (k1 + np.uint64(0xBB67AE85)) & m32
-    return c0, c1, c2, c3
-
-
-def _box_muller(a, b, fp64):
-    """u1 = (a + 1/2) 2^-32; u2 from all 32 bits of b (FP64 path) or its top 23 (FP32)."""
-    u1 = (a.astype(np.float64) + 0.5) * 2.0 ** -32
-    u2 = b.astype(np.float64) * 2.0 ** -32 if fp64 else (b >> np.uint64(9)).astype(np.float64) * 2.0 ** -23
-    rad = np.sqrt(-2.0 * np.log(u1))
-    ang = 2.0 * np.pi * u2 - np.pi
-    return rad * np.cos(ang), rad * np.sin(ang)
-
-
-def counter_noise(g, seed, fp64, epoch=0):
-    """The device's seeded noise in the reference draw order (R2C field backend, even last
-    extent): stored frequency s with last-axis index kl < T/2 takes words (x, y) of
-    Philox(s, 0, 'pair', 0); its partner kl + T/2 takes words (z, w) of the same call."""
-    dim = g.dim
-    T = [g.T[i] for i in range(3)]
-    T0c = T[0] // 2 + 1
-    Tl = T[dim - 1]
-    h = Tl // 2
-    if dim == 2:
-        k0, kl = np.meshgrid(np.arange(T0c), np.arange(h), indexing="ij")
-        k1 = np.zeros_like(k0)
-    else:
-        k0, k1, kl = np.meshgrid(np.arange(T0c), np.arange(T[1]), np.arange(h), indexing="ij")
-
-    def stored(kk):
-        if dim == 2:
-            return k0 + T0c * kk
-        if g.transposed:
-            return k0 + T0c * (kk + T[2] * k1)
-        return k0 + T0c * (k1 + T[1] * kk)
-
-    s0, s1 = stored(kl).ravel(), stored(kl + h).ravel()
-    x, y, z, w = _philox4x32_10((s0, np.zeros_like(s0), np.full_like(s0, 0x70616972), np.full_like(s0, epoch)),
-                                seed)
-    out = np.empty(int(g.noise))
-    out[2 * s0], out[2 * s0 + 1] = _box_muller(x, y, fp64)
-    out[2 * s1], out[2 * s1 + 1] = _box_muller(z, w, fp64)
-    return out
-
-
 @pytest.mark.parametrize("prec", [pfb200.PREC_F64, pfb200.PREC_F32])
 @pytest.mark.parametrize("name", ["2d-exp-pow2", "2d-sph-geo-pow2", "3d-matern32-axi-pow2",
                                   "3d-exp-iso-notransp-pow2", "2d-exp-iso", "3d-matern32-axi"])
@@ -402,6 +363,25 @@ def test_ensemble_matches_single_field_oracle(oracle):
             ref, _ = oracle.generate(d, lam, counter_noise(g, 777 + i, False, epoch=call))
             assert rel(E.field(out, i), ref) < TOL32, (call, i)
     E.close()
+
+
+def test_ensemble_autotune_keeps_parity(oracle):
+    """Measured planning of every field changes kernel choices only: after it (and a new
+    capture) each field still equals the oracle on its reproduced counters."""
+    pfb200.wisdom_forget()
+    descs = [desc_of(c, precision=pfb200.PREC_F32) for c in ENSEMBLE[:4]]
+    E = pfb200.Ensemble(descs, seed=99)
+    E.spectra()
+    E.generate()  # captured before tuning: the tuner drops this graph
+    assert E.autotune(repetitions=1) == len(descs)
+    out = E.generate()  # call 2 of this ensemble
+    for i, d in enumerate(descs):
+        g = oracle.resolve(d)
+        lam, _, _ = oracle.spectrum(d)
+        ref, _ = oracle.generate(d, lam, counter_noise(g, 99 + i, False, epoch=2))
+        assert rel(E.field(out, i), ref) < TOL32, i
+    E.close()
+    pfb200.wisdom_forget()
 
 
 def test_ensemble_device_replay_is_new_noise(oracle):
@@ -470,11 +450,35 @@ def test_dctdst_seeded_covariance(oracle):
     P.close()
 
 
-def test_dctdst_rejects_matvec_and_transposed():
-    d = desc_of(DCTDST["2d-exp-iso"], transposed=0, field_backend=pfb200.FIELD_DCTDST)
+@pytest.mark.parametrize("prec", [pfb200.PREC_F64, pfb200.PREC_F32])
+@pytest.mark.parametrize("name", list(DCTDST))
+def test_dctdst_matvec_parity(oracle, name, prec):
+    """Products of the DCT/DST field backend (matrix.hh:1449-1473, one r2r product per
+    symmetry type, summed) equal the circulant product (C_ext x)/N on the domain, which the
+    oracle computes through the R2C field backend with the same DCT eigenvalues."""
+    d, dr = _dctdst_descs(DCTDST[name], prec)
+    lam, _, _ = oracle.spectrum(dr)
+    g = oracle.resolve(dr)
     P = pfb200.Plan(d)
-    with pytest.raises(pfb200.PfError):
-        P.matvec(np.zeros(P.info.domain_size))
+    P.spectrum_build()
+    x = np.random.default_rng(8).standard_normal(g.domain)
+    dt = np.float64 if prec == pfb200.PREC_F64 else np.float32
+    for op in (pfb200.OP_MUL, pfb200.OP_ROOT, pfb200.OP_INVEXT):
+        # 1/lambda amplifies the rounding of tiny eigenvalues (condition number of the torus)
+        if op == pfb200.OP_INVEXT and lam.min() < 1e-6 * lam.max():
+            continue
+        out = P.matvec(x.astype(dt), op=op, precision=prec)
+        assert rel(out, oracle.matvec(dr, lam, op, x)) < (TOL64 if prec == pfb200.PREC_F64 else TOL32), op
+    if name == "2d-exp-iso":
+        # CG on the DCT/DST plan: the same operator, so the residual-mode solve converges
+        b = np.random.default_rng(9).standard_normal(g.domain)
+        xs, rep = P.multiply_inverse(b, mode=pfb200.CG_RESIDUAL, tolerance=1e-8)
+        assert rep["relative_residual"] <= 1e-8
+        assert rel(oracle.matvec(dr, lam, pfb200.OP_MUL, xs), b) <= 1.1e-8
+    P.close()
+
+
+def test_dctdst_rejects_transposed():
     with pytest.raises(pfb200.PfError):
         pfb200.Plan(desc_of(DCTDST["2d-exp-iso"], field_backend=pfb200.FIELD_DCTDST))
 
@@ -530,4 +534,34 @@ def test_pipelined_batch_to_host_equals_device_batch():
     host = torch.empty(4 * n, dtype=torch.float32).pin_memory().numpy()
     P.generate_batch(seed=9, count=4, out=host)
     assert np.array_equal(host, dev.cpu().numpy())
+    P.close()
+
+
+@pytest.mark.parametrize("lanes", [1, 3])
+@pytest.mark.parametrize("mode", [pfb200.CG_REFERENCE, pfb200.CG_RESIDUAL])
+def test_cg_batch_lanes_equal_single_solves(oracle, mode, lanes):
+    """pf_multiply_inverse_batch: every right-hand side gets the solution and report of a
+    single pf_multiply_inverse call (same deterministic reductions), whichever lane runs
+    it; host and device buffers."""
+    torch = pytest.importorskip("torch")
+    # reference mode starts from the torus inverse 1/lambda, which is infinite where the
+    # clamped configurations have zero eigenvalues (in the reference too): a config without
+    name = "3d-gexp-iso-notransp" if mode == pfb200.CG_REFERENCE else "3d-matern32-axi"
+    d, P, lam, st, _ = plan_and_oracle(oracle, CONFIGS[name], cg_iterations=80)
+    g = oracle.resolve(d)
+    B = np.random.default_rng(21).standard_normal((5, g.domain))
+    B[2] = 0.0  # the zero-field shortcut inside a batch
+    kw = dict(mode=mode, tolerance=1e-8, inner_fp32=True)
+    singles = [P.multiply_inverse(B[i], **kw) for i in range(5)]
+    X, reps = P.multiply_inverse_batch(B, lanes=lanes, **kw)
+    for i in range(5):
+        assert rel(X[i], singles[i][0]) <= 1e-14 if B[i].any() else not X[i].any(), i
+        assert reps[i]["iterations"] == singles[i][1]["iterations"], i
+    if mode == pfb200.CG_RESIDUAL:
+        assert max(r["relative_residual"] for r in reps) <= 1e-8
+    Bd = torch.from_numpy(B).cuda()
+    Xd = torch.empty_like(Bd)
+    P.multiply_inverse_batch(Bd, Xd, lanes=lanes, **kw)
+    torch.cuda.synchronize()
+    assert rel(Xd.cpu().numpy(), X) <= 1e-14
     P.close()

@@ -205,7 +205,7 @@ def test_dctdst_oracle_covariance_equals_circulant_embedding(oracle):
 def test_host_philox_known_answer():
     """The host reproduction of the device's counter-based generator (used to check seeded
     generation) is Philox4x32-10: known-answer vector for counter 0, key 0 (Salmon et al.)."""
-    from test_gpu_parity import _philox4x32_10
+    from helpers import _philox4x32_10
     z = np.zeros(1, dtype=np.uint64)
     assert [int(v[0]) for v in _philox4x32_10((z, z, z, z), 0)] == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
 
