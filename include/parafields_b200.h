@@ -66,7 +66,10 @@ typedef enum pf_covariance {
   PF_COV_CAUCHY = 9,
   PF_COV_GENERALIZED_CAUCHY = 10,
   PF_COV_CUBIC = 11,
-  PF_COV_WHITE_NOISE = 12
+  PF_COV_WHITE_NOISE = 12,
+  /* "custom-iso" / "custom-aniso": the matrix comes from the caller's covariance values,
+   * pf_spectrum_build_values (matrix.hh:223-230) */
+  PF_COV_CUSTOM = 13
 } pf_covariance;
 
 /* stochastic.anisotropy (matrix.hh:479-493) */
@@ -250,6 +253,19 @@ pf_status pf_plan_get_info(const pf_plan* plan, pf_plan_info* info);
  * rule (PF_ERR_NEG_EIGEN unless desc.approximate). `stats` may be NULL. */
 pf_status pf_spectrum_build(pf_plan* plan, pf_eig_stats* stats);
 
+/* Matrix::fillTransformedMatrix(Covariance&&) with a covariance functor of the caller's
+ * own (matrix.hh:223-265, the "custom-iso"/"custom-aniso" covariances that
+ * RandomField::fillMatrix passes in, randomfield.hh:430-451): the caller evaluates its
+ * functor on the host at the matrix cells and hands over the values; the rest is
+ * pf_spectrum_build (FP64 transform with the /N scaling, eigenvalue scan, clamp,
+ * NegativeEigenvalueError rule).  `values` (memory `mem`) holds one value per matrix
+ * cell, dimension 0 fastest, in the natural (untransposed) order: prod(T_i/2+1) cells
+ * (index i_d in [0, T_d/2]) for the DCT matrix backend, prod(T_i) for R2C and DFT; cell
+ * index i_d stands for the coordinate i_d * h_d, minus T_d * h_d beyond half the torus
+ * (matrix.hh:615-638).  PF_ERR_ARG when `count` differs from that cell count. */
+pf_status pf_spectrum_build_values(pf_plan* plan, const double* values, uint64_t count, int32_t mem,
+                                   pf_eig_stats* stats);
+
 /* Copies the finalized eigenvalues (FP64) in the reference's storage layout
  * (DCT: prod(T_i/2+1); R2C: N_c real parts; DFT: N real parts). */
 pf_status pf_spectrum_copy(pf_plan* plan, double* out, uint64_t count);
@@ -294,6 +310,11 @@ pf_status pf_ensemble_spectra(pf_ensemble* ensemble, pf_eig_stats* stats, int32_
  * them in the device buffer of pf_ensemble_device_output).  The first call captures the
  * graph; every call is one graph launch.  Synchronous. */
 pf_status pf_ensemble_generate(pf_ensemble* ensemble, void* out, int32_t out_mem);
+/* Measured planning (pf_plan_autotune) of every field's realization passes, after
+ * pf_ensemble_spectra; fields of one geometry share one timing through the wisdom table.
+ * `timed` (may be NULL) receives the number of fields that were timed.  A graph captured
+ * earlier is dropped and recaptured with the tuned kernels by the next generate call. */
+pf_status pf_ensemble_autotune(pf_ensemble* ensemble, int32_t repetitions, int32_t* timed);
 /* Replays the captured graph on `stream` (a cudaStream_t used as given; 0 is the legacy
  * default stream) without waiting. */
 pf_status pf_ensemble_launch(pf_ensemble* ensemble, void* stream);
@@ -310,17 +331,20 @@ pf_status pf_matvec(pf_plan* plan, int32_t op, int32_t precision, const void* in
 
 /* FP64 matrix-vector product (as pf_matvec with PF_PREC_F64) that allocates no memory.
  * No counterpart in the reference: it exists for callers that may not call cudaMalloc
- * when they need the product -- code living inside another framework's memory pool,
+ * when they need the product -- code living inside another framework's memory pool, and
  * solvers that reserve all device memory at start-up and cannot afford the device
- * synchronization of a later allocation, and callbacks that run during stream capture.
- * Limits: 2D plans with the R2C field backend, spectrum already built (PF_ERR_STATE
- * otherwise), `in`/`out` are device pointers of prod(cells) doubles, and the scratch
+ * synchronization of a later allocation.
+ * Limits: 2D plans with the R2C field backend (PF_ERR_CONFIG otherwise), spectrum already
+ * built (PF_ERR_STATE otherwise); `in`/`out` are device pointers of prod(cells) doubles on
+ * the plan's GPU, which must be the current device (PF_ERR_ARG otherwise); the scratch
  * (T0/2+1)*n1 + T0/2 + T0 + T1 complex doubles must fit in the library's fixed
- * 2^18-element (4 MiB) device array (PF_ERR_ARG otherwise).  That array lives in every
- * GPU that loads the library until the process exits; the first call on a device looks
- * up its address (make that call before any stream capture).  Calls share the array:
- * calls that overlap on the GPU race and must be serialized.  Asynchronous on the plan's
- * stream. */
+ * 2^18-element (4 MiB) device array (PF_ERR_ARG otherwise); torus lengths with a prime
+ * factor above 13 (no Bluestein transform on this path) and rows whose transform tile
+ * exceeds 227 KiB of shared memory return PF_ERR_CONFIG (pf_matvec serves both).
+ * The array lives in every GPU that loads the library until the process exits; the first
+ * call on a device looks up its address (make that call before any stream capture).
+ * Calls share the array: calls that overlap on the GPU race and must be serialized.
+ * Asynchronous on the plan's stream. */
 pf_status pf_matvec_static(pf_plan* plan, int32_t op, const double* in, double* out);
 
 /* Matrix::multiplyInverse (matrix.hh:189-206): zero-input shortcut, torus-inverse
@@ -328,6 +352,17 @@ pf_status pf_matvec_static(pf_plan* plan, int32_t op, const double* in, double* 
  * FP64 vectors; `opts` NULL = reference mode. */
 pf_status pf_multiply_inverse(pf_plan* plan, const double* b, double* x, int32_t mem,
                               const pf_cg_opts* opts, pf_cg_report* report);
+
+/* Matrix::multiplyInverse (matrix.hh:189-206) for `count` right-hand sides stored back to
+ * back in B (prod(cells) doubles each, memory `mem`), solutions into X, one report per
+ * right-hand side in `reports` (may be NULL).  Each solve is the computation of
+ * pf_multiply_inverse on that right-hand side; up to `lanes` (1..8) solves run at once,
+ * each on its own stream with its own workspaces (about 14 domain-sized FP64 vectors of
+ * device memory per lane) sharing the plan's spectrum, so one solve's reductions and
+ * host synchronizations overlap the others' transforms.  With a learned preconditioner
+ * attached the solves run one at a time.  Synchronous. */
+pf_status pf_multiply_inverse_batch(pf_plan* plan, const double* B, double* X, int32_t count, int32_t mem,
+                                    const pf_cg_opts* opts, pf_cg_report* reports, int32_t lanes);
 
 /* Learned boundary correction of the CG preconditioner.  No counterpart in the reference
  * (its innerCG preconditions with the torus inverse only, matrix.hh:1315-1432).  The

@@ -11,9 +11,11 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <map>
 #include <tuple>
 #include <mutex>
+#include <thread>
 #include <type_traits>
 #include <string>
 #include <vector>
@@ -138,7 +140,9 @@ static pf_status resolve(const pf_field_desc* d, Geom* g) {
     g->C[i] = mb == PF_MATRIX_DCT ? g->T[i] / 2 + 1 : (mb == PF_MATRIX_R2C ? (i == 0 ? g->T0c : g->T[i]) : g->T[i]);
   if (g->N > 0xffffffffull) return fail(PF_ERR_CONFIG, "extended domain exceeds 2^32 cells");
   const int c = d->covariance;
-  if (c < 0 || c > PF_COV_WHITE_NOISE) return fail(PF_ERR_CONFIG, "covariance structure not known");
+  if (c < 0 || c > PF_COV_CUSTOM) return fail(PF_ERR_CONFIG, "covariance structure not known");
+  if (c == PF_COV_CUSTOM && d->periodization != PF_PERIODIZATION_CLASSICAL)
+    return fail(PF_ERR_CONFIG, "custom covariance values take embedding.periodization = classical only");
   if (c == PF_COV_GAMMA_EXPONENTIAL && (d->exp_gamma < 0. || d->exp_gamma > 2.))
     return fail(PF_ERR_CONFIG, "exponent gamma has to be between 0 and 2");
   if (c == PF_COV_MATERN && d->matern_nu < 0.) return fail(PF_ERR_CONFIG, "matern nu has to be positive");
@@ -248,6 +252,10 @@ struct pf_plan {
   cudaEvent_t lane_ev[3] = {nullptr, nullptr, nullptr};
   void* ws_b[2] = {nullptr, nullptr};
   size_t ws_b_bytes[2] = {0, 0};
+  // batched CG solves: solver lanes, each a plan that shares this plan's spectrum and
+  // factor arrays (shared = true: it frees only its own workspaces, scratch and stream)
+  bool shared = false;
+  std::vector<pf_plan*> lanes;
 };
 
 static pf_status dalloc(pf_plan* P, void** p, size_t bytes) {
@@ -852,9 +860,16 @@ static pf_status spectrum_alloc(pf_plan* P) {
   return PF_OK;
 }
 
-static pf_status build_spectrum(pf_plan* P) {
+// vals != NULL: the matrix cells were computed by the caller (device array, dimension 0
+// fastest: prod(T_i/2+1) values for the DCT matrix, prod(T_i) otherwise) and replace the
+// covariance evaluation of the first pass; periodization is then the caller's
+static pf_status build_spectrum(pf_plan* P, const double* vals = nullptr) {
   const Geom& g = P->g;
   const pf_field_desc* d = &P->desc;
+  for (pf_plan* l : P->lanes) pf_plan_destroy(l);  // they share the factor arrays freed below
+  P->lanes.clear();
+  if (!vals && d->covariance == PF_COV_CUSTOM)  // matrix.hh:227-230
+    return fail(PF_ERR_STATE, "you need to call fillMatrix with your covariance class as parameter");
   TRY(spectrum_alloc(P));
   for (int a = 0; a < 2; a++)
     for (int o = 0; o < 4; o++)
@@ -866,7 +881,7 @@ static pf_status build_spectrum(pf_plan* P) {
   CovRowLoad cl;
   cl.c = cov_params(d, g);
   const int dim = g.dim;
-  if (d->periodization == PF_PERIODIZATION_COFOLD) {
+  if (d->periodization == PF_PERIODIZATION_COFOLD && !vals) {
     // statistics of the classical values over the matrix cells, then alpha, beta and the
     // offset on the device; the spectrum passes below apply the value map
     if (!P->cof) TRY(dalloc(P, (void**)&P->cof, 6 * sizeof(double)));
@@ -898,8 +913,13 @@ static pf_status build_spectrum(pf_plan* P) {
     const int D1 = dim >= 2 ? g.T[1] / 2 + 1 : 1, D2 = dim >= 3 ? g.T[2] / 2 + 1 : 1;
     const long long rows = (long long)D1 * D2;
     cl.rowmod = D1;
-    TRY((run_freal<double, true>(P, "spec_r2c_cov", g.T[0], T0c, rows, cl, arr_store<double2>(P, A, 1, 0, T0c),
-                                 rows * T0c * 16.0)));
+    if (vals)
+      TRY((run_freal<double, true>(P, "spec_r2c_vals", g.T[0], T0c, rows,
+                                   ValRowLoad{vals, g.T[0], T0c, 1, (unsigned long long)g.D},
+                                   arr_store<double2>(P, A, 1, 0, T0c), rows * T0c * 24.0)));
+    else
+      TRY((run_freal<double, true>(P, "spec_r2c_cov", g.T[0], T0c, rows, cl, arr_store<double2>(P, A, 1, 0, T0c),
+                                   rows * T0c * 16.0)));
     spec = (double2*)A;
     if (dim >= 2) {
       MirrorLoad<double2> ml{(const double2*)A, (unsigned)T0c, (unsigned)((long long)T0c * D1), 1u,
@@ -923,8 +943,13 @@ static pf_status build_spectrum(pf_plan* P) {
     const int T0c = g.T0c;
     const long long rows = (long long)(g.N / (uint64_t)g.T[0]);
     // dimension 0: covariance evaluation fused into the R2C load
-    TRY((run_freal<double, true>(P, "spec_r2c_cov", g.T[0], T0c, rows, cl, arr_store<double2>(P, A, 1, 0, T0c),
-                                 rows * T0c * 16.0)));
+    if (vals)
+      TRY((run_freal<double, true>(P, "spec_r2c_vals", g.T[0], T0c, rows,
+                                   ValRowLoad{vals, g.T[0], g.T[0], 0, (unsigned long long)g.N},
+                                   arr_store<double2>(P, A, 1, 0, T0c), rows * (T0c * 16.0 + g.T[0] * 8.0))));
+    else
+      TRY((run_freal<double, true>(P, "spec_r2c_cov", g.T[0], T0c, rows, cl, arr_store<double2>(P, A, 1, 0, T0c),
+                                   rows * T0c * 16.0)));
     spec = (double2*)A;
     if (dim >= 2) {
       const int L1 = g.T[1], L1o = dct ? g.T[1] / 2 + 1 : g.T[1];
@@ -946,8 +971,13 @@ static pf_status build_spectrum(pf_plan* P) {
     }
   } else {  // DFT matrix: complex torus, every axis complex (dftmatrixbackend.hh:209-238)
     const long long rows = (long long)(g.N / (uint64_t)g.T[0]);
-    TRY((run_pass<double, true>(P, "spec_c2c_d0", g.T[0], g.T[0], rows, 1, -1, -1, cl, NoMid(),
-                                arr_store<double2>(P, A, 1, 0, g.T[0]), rows * g.T[0] * 16.0)));
+    if (vals)
+      TRY((run_pass<double, true>(P, "spec_c2c_d0", g.T[0], g.T[0], rows, 1, -1, -1,
+                                  ValRowLoad{vals, g.T[0], g.T[0], 0, (unsigned long long)g.N}, NoMid(),
+                                  arr_store<double2>(P, A, 1, 0, g.T[0]), rows * g.T[0] * 24.0)));
+    else
+      TRY((run_pass<double, true>(P, "spec_c2c_d0", g.T[0], g.T[0], rows, 1, -1, -1, cl, NoMid(),
+                                  arr_store<double2>(P, A, 1, 0, g.T[0]), rows * g.T[0] * 16.0)));
     spec = (double2*)A;
     void* src = A;
     void* dst = Bw;
@@ -1095,7 +1125,9 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
   // output pruned to the domain extent n_last (pencils: k0 x k1)
   const long long outer = g.dim == 3 ? g.T[1] : 1;
   const long long jst = g.dim == 3 ? (long long)P0 * g.T[1] : P0;
-  const double b1 = (double)T0c * outer * (Tl * (noise_b + lam_b) + (double)g.n[last] * e);
+  // compulsory bytes: the spectrum read once (mirrored and repeated reads of a stored
+  // eigenvalue hit L2), the noise buffer if any, the kept output planes written once
+  const double b1 = (double)g.S * lam_b + (double)T0c * outer * (Tl * noise_b + (double)g.n[last] * e);
   constexpr bool F32 = std::is_same<T, float>::value && std::is_same<S, float>::value;
   struct CapReset {
     pf_plan* P;
@@ -1265,7 +1297,7 @@ static MultMid mult_mid(pf_plan* P, const T* fac) {
   MultMid m{};
   m.dim = g.dim;
   for (int i = 0; i < 3; i++) m.ext[i] = g.T[i];
-  m.C0 = g.fb == PF_FIELD_R2C ? g.T0c : g.T[0];
+  m.C0 = g.fb == PF_FIELD_DFT ? g.T[0] : g.T0c;  // column count of the r2c schedule's half spectrum
   m.layout = g.mb == PF_MATRIX_DCT ? 0 : (g.mb == PF_MATRIX_R2C ? 1 : 2);
   m.LC0 = g.mb == PF_MATRIX_R2C ? g.T0c : g.T[0];
   m.D0 = g.T[0] / 2 + 1;
@@ -1377,11 +1409,16 @@ static pf_status matvec_dft(pf_plan* P, int op, const S* in, S* out) {
                            (double)rows * (g.T[0] * e + g.n[0] * sizeof(S)));
 }
 
+// The DCT/DST field backend's products (matrix.hh:1449-1473) split the zero-padded input
+// into its 2^d even/odd components (setComponent, dctdstfieldbackend.hh:444-460: value /
+// 2^(d - border), zero on an odd axis's border), multiply each by the eigenvalues through
+// its REDFT00/RODFT00 transforms and add the restrictions.  The circulant covariance maps
+// each symmetry class to itself and the components sum to the zero-padded input, so the
+// result is the circulant product (C_ext x)/N restricted to the domain: the r2c schedule
+// computes it in one pass set instead of 2^d.
 template <typename T, typename S>
 static pf_status matvec_dev(pf_plan* P, int op, const S* in, S* out) {
-  if (P->g.fb == PF_FIELD_DCTDST)
-    return fail(PF_ERR_CONFIG, "matrix-vector products with DCTDSTFieldBackend are not supported");
-  if (P->g.fb == PF_FIELD_R2C) return matvec_r2c<T, S>(P, op, in, out);
+  if (P->g.fb == PF_FIELD_R2C || P->g.fb == PF_FIELD_DCTDST) return matvec_r2c<T, S>(P, op, in, out);
   return matvec_dft<T, S>(P, op, in, out);
 }
 
@@ -1498,6 +1535,18 @@ pf_status pf_plan_create(const pf_field_desc* desc, pf_plan** plan) {
 void pf_plan_destroy(pf_plan* P) {
   if (!P) return;
   cudaStreamSynchronize(P->stream);
+  for (pf_plan* l : P->lanes) pf_plan_destroy(l);
+  P->lanes.clear();
+  if (P->shared) {  // a solver lane: the spectrum and factor arrays belong to its parent
+    P->lam64 = nullptr;
+    P->sq64 = nullptr;
+    P->sq32 = nullptr;
+    P->lam32 = nullptr;
+    P->scan = nullptr;
+    P->cof = nullptr;
+    for (int a = 0; a < 2; a++)
+      for (int o = 0; o < 4; o++) P->fac[a][o] = nullptr;
+  }
   void** bufs[] = {(void**)&P->lam64, (void**)&P->sq64, (void**)&P->sq32, (void**)&P->lam32, (void**)&P->scan,
                    (void**)&P->cof, &P->ws[0], &P->ws[1], &P->ws[2], (void**)&P->noise_dev, &P->io_dev, &P->io2_dev, &P->spare};
   for (void** b : bufs)
@@ -1552,6 +1601,35 @@ pf_status pf_spectrum_build(pf_plan* P, pf_eig_stats* stats) {
   if (!P) return fail(PF_ERR_ARG, "null plan");
   P->spare_valid = false;
   pf_status st = build_spectrum(P);
+  if (stats) *stats = P->stats;
+  return check_bounds(P, st);
+}
+
+pf_status pf_spectrum_build_values(pf_plan* P, const double* values, uint64_t count, int32_t mem,
+                                   pf_eig_stats* stats) {
+  if (!P || !values) return fail(PF_ERR_ARG, "null argument");
+  const Geom& g = P->g;
+  const uint64_t need = g.mb == PF_MATRIX_DCT ? g.D : g.N;
+  if (count != need)
+    return fail(PF_ERR_ARG, "covariance values: %llu given, the matrix has %llu cells", (unsigned long long)count,
+                (unsigned long long)need);
+  P->spare_valid = false;
+  const double* dv = values;
+  double* staged = nullptr;
+  if (mem != PF_MEM_DEVICE) {
+    TRY(dalloc(P, (void**)&staged, need * 8));
+    const cudaError_t e = cudaMemcpyAsync(staged, values, need * 8, cudaMemcpyHostToDevice, P->stream);
+    if (e != cudaSuccess) {
+      dfree(P, (void**)&staged, need * 8);
+      return fail(PF_ERR_CUDA, "copy of the covariance values: %s", cudaGetErrorString(e));
+    }
+    dv = staged;
+  }
+  pf_status st = build_spectrum(P, dv);
+  if (staged) {
+    cudaStreamSynchronize(P->stream);
+    dfree(P, (void**)&staged, need * 8);
+  }
   if (stats) *stats = P->stats;
   return check_bounds(P, st);
 }
@@ -1749,6 +1827,22 @@ pf_status pf_multiply_inverse(pf_plan* P, const double* b, double* x, int32_t me
   return check_bounds(P, st);
 }
 
+pf_status pf_multiply_inverse_batch(pf_plan* P, const double* B, double* X, int32_t count, int32_t mem,
+                                    const pf_cg_opts* opts, pf_cg_report* reports, int32_t lanes) {
+  if (!P || (count > 0 && (!B || !X)) || count < 0) return fail(PF_ERR_ARG, "bad argument");
+  if (count == 0) return PF_OK;
+  TRY(ensure_spectrum(P));
+  pf_cg_opts o;
+  if (opts)
+    o = *opts;
+  else {
+    memset(&o, 0, sizeof(o));
+    o.mode = PF_CG_REFERENCE;
+    o.precondition = 1;
+  }
+  return check_bounds(P, cg_solve_batch(P, B, X, count, mem, o, reports, lanes));
+}
+
 pf_status pf_apply_transform(pf_plan* P, int32_t precision, void* data, uint64_t count, int32_t mem) {
   if (!P || !data) return fail(PF_ERR_ARG, "null argument");
   const size_t es = precision == PF_PREC_F64 ? 8 : 4;
@@ -1824,11 +1918,11 @@ const char* pf_version(void) { return "parafields-b200 0.1 (sm_100a)"; }
 //
 // Some callers cannot allocate device memory at the moment they need a product with
 // the covariance: code running inside another framework's memory pool (which may
-// own all of the GPU's memory), solvers that reserve their memory once at start-up
-// and treat a later cudaMalloc as an error because it synchronizes the device, or
-// callbacks that run while a stream is being captured.  For them this variant of
-// the 2D matvec keeps its scratch (the half-spectrum torus and the twiddle tables)
-// in one fixed array that is part of the library image, so a call allocates nothing.
+// own all of the GPU's memory), and solvers that reserve their memory once at start-up
+// and treat a later cudaMalloc as an error because it synchronizes the device.  For
+// them this variant of the 2D matvec keeps its scratch (the half-spectrum torus and the
+// twiddle tables) in one fixed array that is part of the library image, so a call
+// allocates nothing.
 //
 // The array is a file-scope __device__ symbol: every GPU that loads the library holds
 // it until the process exits.  Its host-side name is only a stand-in, so the device
@@ -1844,9 +1938,12 @@ static __device__ __align__(256) double2 g_static_scratch[kStaticScratchElems];
 static std::mutex g_static_mutex;
 static double2* g_static_addr[128] = {nullptr};
 
-static pf_status static_scratch_address(double2** out) {
+static pf_status static_scratch_address(int plan_device, double2** out) {
   int dev = 0;
   CK(cudaGetDevice(&dev));
+  if (dev != plan_device)
+    return fail(PF_ERR_ARG, "pf_matvec_static: the plan's device (%d) must be the current device (%d)", plan_device,
+                dev);
   if (dev < 0 || dev >= 128) return fail(PF_ERR_ARG, "device index %d out of range", dev);
   std::lock_guard<std::mutex> lock(g_static_mutex);
   if (!g_static_addr[dev]) {
@@ -1900,6 +1997,18 @@ extern "C" pf_status pf_matvec_static(pf_plan* P, int32_t op, const double* in, 
   if (g.dim != 2 || g.fb != PF_FIELD_R2C)
     return fail(PF_ERR_CONFIG, "pf_matvec_static serves 2D plans with the R2C field backend");
   if (!P->have_spec) return fail(PF_ERR_STATE, "spectrum not built: call pf_spectrum_build first");
+  // the kernels only reach device memory of the plan's GPU: anything else is refused
+  // here instead of faulting inside a kernel
+  for (const void* p : {(const void*)in, (const void*)out}) {
+    cudaPointerAttributes at{};
+    const cudaError_t e = cudaPointerGetAttributes(&at, p);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(PF_ERR_ARG, "pf_matvec_static: in/out must be device pointers (%s)", cudaGetErrorString(e));
+    }
+    if ((at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != P->device)
+      return fail(PF_ERR_ARG, "pf_matvec_static: in/out must be device memory of the plan's GPU %d", P->device);
+  }
   const int T0 = g.T[0], T1 = g.T[1], L0 = T0 / 2, T0c = g.T0c, n0 = g.n[0], n1 = g.n[1];
   const size_t nX = (size_t)T0c * n1;
   const size_t need = nX + (size_t)L0 + (size_t)T0 + (size_t)T1;
@@ -1907,7 +2016,7 @@ extern "C" pf_status pf_matvec_static(pf_plan* P, int32_t op, const double* in, 
     return fail(PF_ERR_ARG, "field too large for the static scratch: needs %zu complex doubles, limit %zu", need,
                 kStaticScratchElems);
   double2* base = nullptr;
-  TRY(static_scratch_address(&base));
+  TRY(static_scratch_address(P->device, &base));
   double2* X = base;
   double2* twL = X + nX;
   double2* twT = twL + L0;

@@ -32,6 +32,9 @@ enum CgSlot {
   S_RR = 7,     // r . r
   S_BB = 8,     // b . b
   S_NZ = 9,     // count of |b_i| > 1e-10
+  S_DONE = 10,  // residual-mode inner solve: 0 running, 1 converged, 2 NaN residual
+  S_ITERS = 11, // residual-mode inner solve: iterations counted until it stopped
+  S_THR = 12,   // residual-mode inner solve: stop once r . r <= S_THR
   S_COUNT = 16
 };
 
@@ -109,8 +112,10 @@ __global__ void k_finish(const double* part, int nblk, int nout, double* s, int 
   }
 }
 
-// beta = SPNEW / SP (matrix.hh:1409-1417); SP <- SPNEW
+// beta = SPNEW / SP (matrix.hh:1409-1417); SP <- SPNEW.  Nothing once the inner solve
+// stopped (S_DONE is never set in reference mode).
 __global__ void k_cg_beta(double* s) {
+  if (s[S_DONE] != 0.) return;
   s[S_BETA] = s[S_SPNEW] / s[S_SP];
   s[S_SP] = s[S_SPNEW];
 }
@@ -118,6 +123,7 @@ __global__ void k_cg_beta(double* s) {
 // d = z + beta d
 __global__ void __launch_bounds__(kCgThreads) k_cg_dir(double* __restrict__ d, const double* __restrict__ z, uint64_t n,
                                                        const double* s) {
+  if (s[S_DONE] != 0.) return;
   const double beta = s[S_BETA];
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     d[i] = z[i] + beta * d[i];
@@ -129,11 +135,14 @@ __global__ void k_sub(const double* __restrict__ b, const double* __restrict__ A
     r[i] = b[i] - Ax[i];
 }
 
-// residual-mode PCG update: x += alpha d, r -= alpha Ad (alpha = SP / DEN); part = r . r
+// residual-mode PCG update: x += alpha d, r -= alpha Ad (alpha = SP / DEN); part = r . r.
+// Nothing once the inner solve stopped: the host checks S_DONE only every few
+// iterations, and the iterations launched after the stop leave x and r unchanged.
 __global__ void __launch_bounds__(kCgThreads) k_pcg_update(double* __restrict__ x, double* __restrict__ r,
                                                            const double* __restrict__ d, const double* __restrict__ Ad,
                                                            uint64_t n, const double* s, double* part) {
   __shared__ double sh[32];
+  if (s[S_DONE] != 0.) return;
   const double alpha = s[S_SP] / s[S_DEN];
   double v = 0.;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -144,6 +153,24 @@ __global__ void __launch_bounds__(kCgThreads) k_pcg_update(double* __restrict__ 
   }
   v = block_sum(v, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+// start of a residual-mode inner solve: stop threshold on r . r, counters cleared
+__global__ void k_pcg_start(double* s, double thr) {
+  s[S_DONE] = 0.;
+  s[S_ITERS] = 0.;
+  s[S_THR] = thr;
+}
+
+// after an update: count the iteration, stop on convergence or a NaN residual
+__global__ void k_pcg_check(double* s) {
+  if (s[S_DONE] != 0.) return;
+  s[S_ITERS] += 1.;
+  const double rr = s[S_RR];
+  if (!(rr == rr))
+    s[S_DONE] = 2.;
+  else if (rr <= s[S_THR])
+    s[S_DONE] = 1.;
 }
 
 __global__ void k_axpy(double* __restrict__ y, const double* __restrict__ x, uint64_t n) {

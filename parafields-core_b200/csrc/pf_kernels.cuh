@@ -812,6 +812,28 @@ struct CovRowLoad {
   }
 };
 
+// covariance values computed by the caller (a user covariance functor evaluated on the
+// host, matrix.hh:223-265 "custom-iso"/"custom-aniso") read in place of cov_at: `v` holds
+// the matrix cells with dimension 0 fastest, `rowlen` values per row (T0, or T0/2+1 for
+// the DCT matrix, whose row j > T0/2 reads the mirrored cell T0 - j)
+struct ValRowLoad {
+  const double* v;
+  int T0;
+  int rowlen;
+  int mirror;
+  unsigned long long n;
+  template <typename T>
+  __device__ __forceinline__ T real(long long p, int j) const {
+    const int jj = (mirror && j > T0 / 2) ? T0 - j : j;
+    const unsigned long long i = (unsigned long long)p * (unsigned long long)rowlen + (unsigned long long)jj;
+    return in_bounds((long long)i, (long long)n) ? (T)v[i] : (T)0;
+  }
+  template <typename T>
+  __device__ __forceinline__ cx<T> load(long long p, int j, long long) const {
+    return mk<T>(real<T>(p, j), (T)0);
+  }
+};
+
 // ---------------------------------------------------------------------------
 // counter-based normal noise: Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel
 // random numbers: as easy as 1, 2, 3", SC 2011) + Box-Muller.  One call yields the

@@ -49,70 +49,70 @@ inline void check(pf_status st) {
 // matrix.hh:232-260, 268-269, 479-493, 515-602; covariance.hh:33-128, 395-396, 515-516,
 // 711-713; mutators.hh:139-154).  Additional keys: gpu.precision (double|float, default
 // from RF) and gpu.eigenCheck (corrected|reference).
-template <unsigned dim, typename RF>
-pf_field_desc descFromConfig(const ParameterTree& config) {
+template <unsigned dim, typename RF, typename Config>
+pf_field_desc descFromConfig(const Config& config) {
   pf_field_desc d;
   pf_field_desc_init(&d);
   d.dim = (int32_t)dim;
-  const auto cells = config.get<std::array<unsigned, dim>>("grid.cells");
-  const auto ext = config.get<std::array<double, dim>>("grid.extensions");
+  const auto cells = config.template get<std::array<unsigned, dim>>("grid.cells");
+  const auto ext = config.template get<std::array<double, dim>>("grid.extensions");
   for (unsigned i = 0; i < dim; i++) {
     d.cells[i] = (int32_t)cells[i];
     d.extensions[i] = ext[i];
   }
-  d.variance = config.get<double>("stochastic.variance");
-  const std::string cov = config.get<std::string>("stochastic.covariance");
+  d.variance = config.template get<double>("stochastic.variance");
+  const std::string cov = config.template get<std::string>("stochastic.covariance");
   static const char* names[] = {"exponential", "gaussian", "spherical", "separableExponential", "matern",
                                 "matern32", "matern52", "dampedOscillation", "gammaExponential", "cauchy",
                                 "generalizedCauchy", "cubic", "whiteNoise"};
   d.covariance = -1;
   for (int i = 0; i < 13; i++)
     if (cov == names[i]) d.covariance = i;
-  if (d.covariance < 0 && cov != "custom-iso" && cov != "custom-aniso")
-    throw std::runtime_error{"covariance structure " + cov + " not known"};
-  if (d.covariance == PF_COV_MATERN) d.matern_nu = config.get<double>("stochastic.maternNu");
-  if (d.covariance == PF_COV_GAMMA_EXPONENTIAL) d.exp_gamma = config.get<double>("stochastic.expGamma");
+  if (cov == "custom-iso" || cov == "custom-aniso") d.covariance = PF_COV_CUSTOM;
+  if (d.covariance < 0) throw std::runtime_error{"covariance structure " + cov + " not known"};
+  if (d.covariance == PF_COV_MATERN) d.matern_nu = config.template get<double>("stochastic.maternNu");
+  if (d.covariance == PF_COV_GAMMA_EXPONENTIAL) d.exp_gamma = config.template get<double>("stochastic.expGamma");
   if (d.covariance == PF_COV_GENERALIZED_CAUCHY) {
-    d.cauchy_alpha = config.get<double>("stochastic.cauchyAlpha");
-    d.cauchy_beta = config.get<double>("stochastic.cauchyBeta");
+    d.cauchy_alpha = config.template get<double>("stochastic.cauchyAlpha");
+    d.cauchy_beta = config.template get<double>("stochastic.cauchyBeta");
   }
-  const std::string aniso = config.get<std::string>("stochastic.anisotropy", std::string("none"));
+  const std::string aniso = config.template get<std::string>("stochastic.anisotropy", std::string("none"));
   if (aniso == "none") {
     d.anisotropy = PF_ANISO_NONE;
-    d.corr_length[0] = config.get<double>("stochastic.corrLength");
+    d.corr_length[0] = config.template get<double>("stochastic.corrLength");
   } else if (aniso == "axiparallel") {
     d.anisotropy = PF_ANISO_AXIPARALLEL;
-    const auto c = config.get<std::array<double, dim>>("stochastic.corrLength");
+    const auto c = config.template get<std::array<double, dim>>("stochastic.corrLength");
     for (unsigned i = 0; i < dim; i++) d.corr_length[i] = c[i];
   } else if (aniso == "geometric") {
     d.anisotropy = PF_ANISO_GEOMETRIC;
-    const auto c = config.get<std::array<double, dim * dim>>("stochastic.corrLength");
+    const auto c = config.template get<std::array<double, dim * dim>>("stochastic.corrLength");
     for (unsigned i = 0; i < dim * dim; i++) d.corr_length[i] = c[i];
   } else {
     throw std::runtime_error{"stochastic.anisotropy must be \"none\", \"axiparallel\" or \"geometric\""};
   }
-  d.periodic = config.get<bool>("randomField.periodic", false);
-  d.approximate = config.get<bool>("embedding.approximate", false);
-  d.cg_iterations = (int32_t)config.get<unsigned>("randomField.cgIterations", 100u);
-  d.embedding_factor = (int32_t)config.get<unsigned>("embedding.factor", 2u);
-  d.threshold = config.get<double>("embedding.threshold", 1e-14);
-  if (config.hasKey("fftw.transposed")) d.transposed = config.get<bool>("fftw.transposed") ? 1 : 0;
-  const std::string per = config.get<std::string>("embedding.periodization", std::string("classical"));
+  d.periodic = config.template get<bool>("randomField.periodic", false);
+  d.approximate = config.template get<bool>("embedding.approximate", false);
+  d.cg_iterations = (int32_t)config.template get<unsigned>("randomField.cgIterations", 100u);
+  d.embedding_factor = (int32_t)config.template get<unsigned>("embedding.factor", 2u);
+  d.threshold = config.template get<double>("embedding.threshold", 1e-14);
+  if (config.hasKey("fftw.transposed")) d.transposed = config.template get<bool>("fftw.transposed") ? 1 : 0;
+  const std::string per = config.template get<std::string>("embedding.periodization", std::string("classical"));
   if (per == "merge" || per == "fold" || per == "cofold") {
     d.periodization = per == "merge" ? PF_PERIODIZATION_MERGE
                                      : (per == "fold" ? PF_PERIODIZATION_FOLD : PF_PERIODIZATION_COFOLD);
-    d.fold_max_factor = config.get<double>("embedding.foldMaxFactor", 1.);
-    d.fold_recursions = (int32_t)config.get<unsigned>("embedding.foldRecursions", 99u);
-    d.cofold_max_factor = config.get<double>("embedding.cofoldMaxFactor", 5.);
-    d.cofold_recursions = (int32_t)config.get<double>("embedding.cofoldRecursions", 1.);
-    const std::string sig = config.get<std::string>("embedding.sigmoid", std::string("smoothstep"));
+    d.fold_max_factor = config.template get<double>("embedding.foldMaxFactor", 1.);
+    d.fold_recursions = (int32_t)config.template get<unsigned>("embedding.foldRecursions", 99u);
+    d.cofold_max_factor = config.template get<double>("embedding.cofoldMaxFactor", 5.);
+    d.cofold_recursions = (int32_t)config.template get<double>("embedding.cofoldRecursions", 1.);
+    const std::string sig = config.template get<std::string>("embedding.sigmoid", std::string("smoothstep"));
     if (sig == "smooth")
       d.sigmoid = PF_SIGMOID_SMOOTH;
     else if (sig == "smoothstep")
       d.sigmoid = PF_SIGMOID_SMOOTHSTEP;
     else
       throw std::runtime_error{"embedding.sigmoid must be \"smooth\" or \"smoothstep\""};
-    const std::string comb = config.get<std::string>("stochastic.sigmoidCombine", std::string("radialPlus"));
+    const std::string comb = config.template get<std::string>("stochastic.sigmoidCombine", std::string("radialPlus"));
     if (comb == "radialPlus")
       d.sigmoid_combine = PF_COMBINE_RADIAL_PLUS;
     else if (comb == "radial")
@@ -121,16 +121,16 @@ pf_field_desc descFromConfig(const ParameterTree& config) {
       d.sigmoid_combine = PF_COMBINE_TENSOR;
     else
       throw std::runtime_error{"sigmoidCombine must be tensor, radial or radialPlus"};
-    d.sigmoid_start = config.get<double>("embedding.sigmoidStart", 1.);
-    d.sigmoid_end = config.get<double>("embedding.sigmoidEnd", (double)d.embedding_factor - 1.);
-    d.merge_recursions = (int32_t)config.get<unsigned>("embedding.mergeRecursions", 99u);
+    d.sigmoid_start = config.template get<double>("embedding.sigmoidStart", 1.);
+    d.sigmoid_end = config.template get<double>("embedding.sigmoidEnd", (double)d.embedding_factor - 1.);
+    d.merge_recursions = (int32_t)config.template get<unsigned>("embedding.mergeRecursions", 99u);
   } else if (per != "classical") {
     throw std::runtime_error{
         "stochastic.periodization must be \"classical\", \"merge\", \"fold\", or \"cofold\""};
   }
-  const std::string optim = config.get<std::string>("embedding.optim", std::string("none"));
+  const std::string optim = config.template get<std::string>("embedding.optim", std::string("none"));
   if (optim != "none") throw std::runtime_error{"optimization requires dune-nonlinopt"};
-  const std::string tr = config.get<std::string>("randomField.transform", std::string("none"));
+  const std::string tr = config.template get<std::string>("randomField.transform", std::string("none"));
   if (tr == "none")
     d.transform = PF_TRANSFORM_NONE;
   else if (tr == "logNormal")
@@ -141,13 +141,13 @@ pf_field_desc descFromConfig(const ParameterTree& config) {
     d.transform = PF_TRANSFORM_SIGN;
   else if (tr == "boxCox") {
     d.transform = PF_TRANSFORM_BOXCOX;
-    d.boxcox_lambda = config.get<double>("transform.boxCoxLambda");
+    d.boxcox_lambda = config.template get<double>("transform.boxCoxLambda");
   } else
     throw std::runtime_error{"transform type not known"};
   const std::string prec =
-      config.get<std::string>("gpu.precision", std::string(sizeof(RF) == 4 ? "float" : "double"));
+      config.template get<std::string>("gpu.precision", std::string(sizeof(RF) == 4 ? "float" : "double"));
   d.precision = prec == "float" ? PF_PREC_F32 : PF_PREC_F64;
-  const std::string eig = config.get<std::string>("gpu.eigenCheck", std::string("corrected"));
+  const std::string eig = config.template get<std::string>("gpu.eigenCheck", std::string("corrected"));
   d.eigen_check = eig == "reference" ? PF_EIGCHECK_REFERENCE : PF_EIGCHECK_CORRECTED;
   return d;
 }
@@ -183,9 +183,46 @@ class ValueTransform {
   }
 };
 
-// The Matrix of one field configuration (matrix.hh:55-206) on the GPU.
+// Covariance values of a caller-supplied functor on the matrix cells of a plan, in the
+// layout pf_spectrum_build_values takes: computeMatrixEntriesWithMirroring
+// (matrix.hh:615-638) with the ScaledIdentityMatrix geometry that fillTransformedMatrix
+// applies to user functors (matrix.hh:262-264, covariance.hh:18-44), i.e. coordinate
+// i_d * h_d (minus T_d * h_d beyond half the torus) divided by stochastic.corrLength and
+// value covariance(variance, transformed coordinate).  The DCT matrix keeps the
+// prod(T_d/2+1) non-mirrored cells, the R2C and DFT matrices every torus cell.
+template <unsigned dim, typename RF, typename Covariance>
+std::vector<double> customCovarianceValues(const pf_plan_info& info, const std::array<double, dim>& extensions,
+                                           double variance, double corrLength, Covariance&& covariance) {
+  std::array<std::size_t, 3> m{1, 1, 1};
+  std::array<double, 3> h{1., 1., 1.}, period{1., 1., 1.};
+  for (unsigned i = 0; i < dim; i++) {
+    const unsigned T = (unsigned)info.ext_cells[i];
+    m[i] = info.matrix_backend == PF_MATRIX_DCT ? T / 2 + 1 : T;
+    h[i] = extensions[i] / (double)info.cells[i];
+    period[i] = h[i] * (double)T;  // extensions * embedding factor
+  }
+  std::vector<double> values(m[0] * m[1] * m[2]);
+  std::array<RF, dim> coord, trans;
+  std::size_t k = 0;
+  for (std::size_t i2 = 0; i2 < m[2]; i2++)
+    for (std::size_t i1 = 0; i1 < m[1]; i1++)
+      for (std::size_t i0 = 0; i0 < m[0]; i0++, k++) {
+        const std::size_t idx[3] = {i0, i1, i2};
+        for (unsigned i = 0; i < dim; i++) {
+          coord[i] = (RF)((double)idx[i] * h[i]);
+          if (coord[i] > (RF)(0.5 * period[i])) coord[i] -= (RF)period[i];
+          trans[i] = (RF)(1. / corrLength) * coord[i];
+        }
+        values[k] = (double)covariance((RF)variance, trans);
+      }
+  return values;
+}
+
+// The plan of one field configuration (matrix.hh:55-206) on the GPU, as the facade's
+// RandomField below uses it.  parafields_b200/gpumatrix.hh holds the adapter that fills
+// the reference's own IsoMatrix/AnisoMatrix template slot.
 template <typename RF>
-class GpuMatrix {
+class GpuPlan {
   pf_plan* plan_ = nullptr;
   pf_plan_info info_{};
   pf_field_desc desc_{};
@@ -193,15 +230,15 @@ class GpuMatrix {
   bool custom_ = false;
 
  public:
-  GpuMatrix(const pf_field_desc& d, bool customCovariance = false) : desc_(d), custom_(customCovariance) {
+  GpuPlan(const pf_field_desc& d, bool customCovariance = false) : desc_(d), custom_(customCovariance) {
     if ((d.precision == PF_PREC_F64) != (sizeof(RF) == 8))
       throw std::runtime_error{"gpu.precision must match the field's value type"};
     check(pf_plan_create(&d, &plan_));
     check(pf_plan_get_info(plan_, &info_));
   }
-  ~GpuMatrix() { pf_plan_destroy(plan_); }
-  GpuMatrix(const GpuMatrix&) = delete;
-  GpuMatrix& operator=(const GpuMatrix&) = delete;
+  ~GpuPlan() { pf_plan_destroy(plan_); }
+  GpuPlan(const GpuPlan&) = delete;
+  GpuPlan& operator=(const GpuPlan&) = delete;
 
   const pf_plan_info& info() const { return info_; }
   pf_plan* plan() const { return plan_; }
@@ -211,6 +248,18 @@ class GpuMatrix {
     if (custom_) throw std::runtime_error{"you need to call fillMatrix with your covariance class as parameter"};
     pf_eig_stats s{};
     check(pf_spectrum_build(plan_, &s));
+    spare_pending_ = false;
+    return s;
+  }
+
+  // fillTransformedMatrix(Covariance&&) with a user functor (matrix.hh:223-265): evaluated
+  // on the host at the matrix cells, transformed and checked on the GPU
+  template <unsigned dim, typename Covariance>
+  pf_eig_stats fillTransformedMatrix(const std::array<double, dim>& extensions, Covariance&& covariance) {
+    const std::vector<double> v = customCovarianceValues<dim, RF>(info_, extensions, desc_.variance,
+                                                                  desc_.corr_length[0], covariance);
+    pf_eig_stats s{};
+    check(pf_spectrum_build_values(plan_, v.data(), v.size(), PF_MEM_HOST, &s));
     spare_pending_ = false;
     return s;
   }
@@ -265,7 +314,7 @@ class RandomField {
   ParameterTree config_;
   pf_field_desc desc_;
   ValueTransform<RF> transform_;
-  std::shared_ptr<GpuMatrix<RF>> matrix_;
+  std::shared_ptr<GpuPlan<RF>> matrix_;
   std::vector<RF> data_;
   bool cacheInvMatvec_, cacheInvRootMatvec_;
   bool invMatvecValid_ = true, invRootMatvecValid_ = true;
@@ -331,7 +380,7 @@ class RandomField {
       cells_[i] = cells_[i] * mul / div;
       desc_.cells[i] = (int32_t)cells_[i];
     }
-    matrix_ = std::make_shared<GpuMatrix<RF>>(desc_, custom_);
+    matrix_ = std::make_shared<GpuPlan<RF>>(desc_, custom_);
   }
 
   // RandomField::refine / coarsen (randomfield.hh:880-1018), using the cached matrix-vector
@@ -405,7 +454,7 @@ class RandomField {
     transform_ = ValueTransform<RF>(desc_.transform, (RF)desc_.boxcox_lambda);
     const std::string cov = config.get<std::string>("stochastic.covariance");
     custom_ = cov == "custom-iso" || cov == "custom-aniso";
-    matrix_ = std::make_shared<GpuMatrix<RF>>(desc_, custom_);
+    matrix_ = std::make_shared<GpuPlan<RF>>(desc_, custom_);
     cells_ = config.get<std::array<unsigned, dim>>("grid.cells");
     dataCells_ = cells_;
     ext_ = config.get<std::array<double, dim>>("grid.extensions");
@@ -414,7 +463,17 @@ class RandomField {
     if (cacheInvRootMatvec_) invRootMatvecPart_ = data_;
   }
 
-  GpuMatrix<RF>& matrix() { return *matrix_; }
+  GpuPlan<RF>& matrix() { return *matrix_; }
+
+  // randomfield.hh:430-451: the matrix of a "custom-iso" / "custom-aniso" field from the
+  // caller's covariance functor, RF operator()(RF variance, const std::array<RF, dim>& x);
+  // classical periodization (the built-in covariances also support merge/fold/cofold)
+  template <typename Covariance>
+  void fillMatrix(Covariance&& covariance) {
+    if (desc_.periodization != PF_PERIODIZATION_CLASSICAL)
+      throw std::runtime_error{"custom covariance functors support embedding.periodization = classical only"};
+    matrix_->template fillTransformedMatrix<dim>(ext_, covariance);
+  }
 
   // randomfield.hh:880-887 / 955-961: double (halve) the resolution of the matrix
   void refineMatrix() { resizeMatrix(2, 1); }

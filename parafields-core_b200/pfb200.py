@@ -27,6 +27,8 @@ COVARIANCES = {
     "matern": 4, "matern32": 5, "matern52": 6, "dampedOscillation": 7,
     "gammaExponential": 8, "cauchy": 9, "generalizedCauchy": 10, "cubic": 11,
     "whiteNoise": 12,
+    # the caller supplies the matrix cells (Plan.spectrum_build_values)
+    "custom-iso": 13, "custom-aniso": 13,
 }
 ANISOTROPIES = {"none": 0, "axiparallel": 1, "geometric": 2}
 TRANSFORMS = {"none": 0, "logNormal": 1, "foldedNormal": 2, "sign": 3, "boxCox": 4}
@@ -172,11 +174,13 @@ def lib():
         "pf_plan_get_info": (i32, [vp, C.POINTER(PlanInfo)]),
         "pf_spectrum_build": (i32, [vp, C.POINTER(EigStats)]),
         "pf_spectrum_copy": (i32, [vp, vp, u64]),
+        "pf_spectrum_build_values": (i32, [vp, vp, u64, i32, C.POINTER(EigStats)]),
         "pf_generate": (i32, [vp, vp, i32, u64, vp, i32, i32]),
         "pf_generate_batch": (i32, [vp, u64, i32, vp, i32, i32]),
         "pf_matvec": (i32, [vp, i32, i32, vp, vp, i32]),
         "pf_matvec_static": (i32, [vp, i32, vp, vp]),
         "pf_multiply_inverse": (i32, [vp, vp, vp, i32, C.POINTER(CgOpts), C.POINTER(CgReport)]),
+        "pf_multiply_inverse_batch": (i32, [vp, vp, vp, i32, i32, C.POINTER(CgOpts), C.POINTER(CgReport), i32]),
         "pf_apply_transform": (i32, [vp, i32, vp, u64, i32]),
         "pf_profile_enable": (i32, [vp, i32]),
         "pf_profile_read": (i32, [vp, C.POINTER(KernelTime), i32, C.POINTER(i32)]),
@@ -187,6 +191,7 @@ def lib():
         "pf_ensemble_spectra": (i32, [vp, C.POINTER(EigStats), C.POINTER(i32)]),
         "pf_ensemble_generate": (i32, [vp, vp, i32]),
         "pf_ensemble_launch": (i32, [vp, vp]),
+        "pf_ensemble_autotune": (i32, [vp, i32, C.POINTER(i32)]),
         "pf_ensemble_device_output": (vp, [vp]),
         "pf_ensemble_launches_per_replay": (u64, [vp]),
         "pf_learned_create": (i32, [vp, i32, u64, C.POINTER(vp)]),
@@ -282,6 +287,17 @@ class Plan:
         _check(lib().pf_spectrum_build(self.h, C.byref(st)))
         return st.as_dict()
 
+    def spectrum_build_values(self, values):
+        """fillTransformedMatrix with caller-computed covariance values on the matrix cells
+        (numpy float64 or a torch CUDA float64 tensor)."""
+        if isinstance(values, np.ndarray):
+            values = np.ascontiguousarray(values, dtype=np.float64)
+        ptr, mem = _ptr(values)
+        st = EigStats()
+        n = values.size if isinstance(values, np.ndarray) else values.numel()
+        _check(lib().pf_spectrum_build_values(self.h, ptr, n, mem, C.byref(st)))
+        return st.as_dict()
+
     def spectrum(self):
         out = np.empty(self.info.spectrum_size, dtype=np.float64)
         _check(lib().pf_spectrum_copy(self.h, out.ctypes.data, out.size))
@@ -325,6 +341,21 @@ class Plan:
         _check(lib().pf_multiply_inverse(self.h, bptr, xptr, mem, C.byref(opts), C.byref(rep)))
         return x, {"iterations": rep.iterations, "refinements": rep.refinements,
                    "relative_residual": rep.relative_residual}
+
+    def multiply_inverse_batch(self, B, X=None, lanes=2, mode=CG_REFERENCE, tolerance=1e-8, max_iterations=0,
+                               inner_fp32=False, precondition=True):
+        """count right-hand sides (rows of B, prod(cells) doubles each) solved with up to
+        `lanes` solves in flight; returns (X, list of reports)"""
+        if X is None:
+            X = np.empty_like(B)
+        count = B.shape[0]
+        opts = CgOpts(mode, max_iterations, tolerance, int(inner_fp32), int(precondition))
+        reps = (CgReport * count)()
+        bptr, mem = _ptr(B)
+        xptr, _ = _ptr(X)
+        _check(lib().pf_multiply_inverse_batch(self.h, bptr, xptr, count, mem, C.byref(opts), reps, lanes))
+        return X, [{"iterations": r.iterations, "refinements": r.refinements,
+                    "relative_residual": r.relative_residual} for r in reps]
 
     def apply_transform(self, data, precision=PREC_F64):
         ptr, mem = _ptr(data)
@@ -384,6 +415,12 @@ class Ensemble:
         ptr, mem = _ptr(out)
         _check(lib().pf_ensemble_generate(self.h, ptr, mem))
         return out
+
+    def autotune(self, repetitions=1):
+        """measured planning of every field; returns the number of fields timed"""
+        t = C.c_int32()
+        _check(lib().pf_ensemble_autotune(self.h, repetitions, C.byref(t)))
+        return t.value
 
     def launch(self, stream=None):
         _check(lib().pf_ensemble_launch(self.h, stream))
