@@ -72,8 +72,10 @@ def realization_work(cells, torus):
     c = lambda L: 5.0 * L * math.log2(L)  # noqa: E731
     passes = {"gen_noise_last": c0 * t1 * c(t2),   # last axis, every pencil of the half spectrum
               "gen_c2c_d1": c0 * n2 * c(t1),       # axis 1 on the n2 kept planes
+              "gen_c2c_d1_tma": c0 * n2 * c(t1),
               "gen_c2r_d0": n1 * n2 * 0.5 * c(t0)}  # complex-to-real rows of the kept cells
-    pass_bytes = {"gen_noise_last": sq + w1, "gen_c2c_d1": w1 + w2, "gen_c2r_d0": w2 + out}
+    pass_bytes = {"gen_noise_last": sq + w1, "gen_c2c_d1": w1 + w2, "gen_c2c_d1_tma": w1 + w2,
+                  "gen_c2r_d0": w2 + out}
     return {"compulsory_bytes": sq + out, "flops": 2.5 * N * math.log2(N), "pass_flops": passes,
             "pass_bytes": pass_bytes, "schedule_bytes": sum(pass_bytes.values())}
 
@@ -558,7 +560,8 @@ def run_cinv(args):
     Lp.attach(False)
     print(json.dumps({"metric": f"C^-1 solves/s ({n}^3 exponential, geometric anisotropy, 1e-8 FP64 residual)",
                       "unit": "solves/s", "value": out["plain"]["solves_per_s"], "dtype": "f32 inner / f64 residual",
-                      "eigen": st, "plain": out["plain"], "learned": out["learned"],
+                      "eigen": st, "plain": out["plain"], "plain_one_lane": out["plain_one_lane"],
+                      "learned": out["learned"],
                       "training": {"pairs": K_train, "pair_generation_s": tpairs, "epochs": args.epochs,
                                    "loss": "residual norm" if args.residual_loss else "solution norm",
                                    "lr": args.lr, "train_s": ttrain, "loss_before": loss0,

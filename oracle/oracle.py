@@ -302,7 +302,8 @@ def learned_loss_grad(desc, lam, theta, H, B, X, residual=False):
 # DCTDSTFieldBackend::setType / set / backwardTransform / extendedFieldToField
 # (include/parafields/backends/dctdstfieldbackend.hh:149-165, 326-438, 631-771) driven by
 # Matrix::generateField (include/parafields/matrix.hh:342-367).  scipy.fft.dct/dst of type 1
-# without normalization are FFTW's REDFT00/RODFT00.  fftw.transposed = false.
+# without normalization are FFTW's REDFT00/RODFT00.  With fftw.transposed the draws follow
+# the transposed cell order; the transforms and the field do not depend on the layout.
 # ---------------------------------------------------------------------------
 def dctdst_noise_size(desc):
     dim = desc.dim
@@ -325,10 +326,18 @@ def generate_dctdst(desc, lam, noise):
     shape = tuple(reversed(D))  # numpy order (d-1, ..., 0)
     sq = np.sqrt(np.maximum(np.asarray(lam, dtype=np.float64), 0.0)).reshape(shape)
     Dtot = int(np.prod(D))
+    # draw order: the backend's local cells, dims d-1 and d-2 swapped when fftw.transposed
+    # (default for dim > 1; dctdstfieldbackend.hh:855-871 with matrix.hh:349-360)
+    transposed = dim > 1 and (desc.transposed < 0 or desc.transposed != 0)
+    stored = list(D)
+    if transposed:
+        stored[dim - 1], stored[dim - 2] = stored[dim - 2], stored[dim - 1]
     field = np.zeros(tuple(reversed(n)))
     for t in range(1 << dim):
         odd = [(t >> i) & 1 for i in range(dim)]
-        r = np.asarray(noise[t * Dtot:(t + 1) * Dtot], dtype=np.float64).reshape(shape)
+        r = np.asarray(noise[t * Dtot:(t + 1) * Dtot], dtype=np.float64).reshape(tuple(reversed(stored)))
+        if transposed:
+            r = np.swapaxes(r, 0, 1)
         X = sq * r * 2.0 ** (-dim / 2.0)
         for i in range(dim):
             ax = dim - 1 - i

@@ -106,8 +106,6 @@ static pf_status resolve(const pf_field_desc* d, Geom* g) {
     return fail(PF_ERR_CONFIG, "R2CMatrixBackend cannot serve DFTFieldBackend");
   // matrix.hh:342-347: the DCT/DST field backend needs the DCT matrix backend
   if (fb == PF_FIELD_DCTDST && mb != PF_MATRIX_DCT) return fail(PF_ERR_CONFIG, "DCTDSTFieldBackend requires DCTMatrixBackend");
-  if (fb == PF_FIELD_DCTDST && d->dim > 1 && d->transposed != 0)
-    return fail(PF_ERR_CONFIG, "DCTDSTFieldBackend is supported with fftw.transposed = false only");
   for (int i = 0; i < d->dim; i++)
     if (mb == PF_MATRIX_DCT && (g->T[i] % 2))
       return fail(PF_ERR_CONFIG, "DCTMatrixBackend requires an even number of extended cells per dimension");
@@ -1060,6 +1058,7 @@ static pf_status check_bounds(pf_plan* P, pf_status st) {
     const unsigned int zero = 0;
     CK(cudaMemcpyToSymbolAsync(g_bounds_error, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, P->stream));
     CK(cudaStreamSynchronize(P->stream));
+    if (flag & 2u) return fail(PF_ERR_TIMEOUT, "a kernel's bounded wait for its tile copies gave up");
     return fail(PF_ERR_CUDA, "internal error: a kernel computed an index outside its buffer (access skipped)");
   }
   return st;
@@ -1148,10 +1147,14 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
     TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)P0 * g.n[1] * g.n[2], &W2));
     const double b2 = (double)T0c * g.n[2] * (g.T[1] + g.n[1]) * e;
     P->grid_cap = P->tune_grid[1];
-    if (F32 && P->tune_variant[1] == 0 && p2_length(g.T[1]) && p2_view_ok(W1, P0, (long long)P0 * g.T[1], g.n[2]) &&
-        p2_view_ok(W2, P0, (long long)P0 * g.n[1], g.n[2]))
-      TRY(p2_c2c<+1>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, g.n[2],
-                     p2_load(P, W1, P0, (long long)P0 * g.T[1], g.T[1], T0c),
+    const bool p2ok = F32 && p2_length(g.T[1]) && p2_view_ok(W1, P0, (long long)P0 * g.T[1], g.n[2]) &&
+                      p2_view_ok(W2, P0, (long long)P0 * g.n[1], g.n[2]);
+    const P2ArrLoad l1 = p2_load(P, W1, P0, (long long)P0 * g.T[1], g.T[1], T0c);
+    if (p2ok && P->tune_variant[1] == 2 && p2_tma_ok(P, l1, g.n[2]))  // tiles staged by TMA
+      TRY(p2_c2c_tma<+1>(P, "gen_c2c_d1_tma", g.T[1], g.n[1], T0c, g.n[2], l1,
+                         p2_store(P, W2, P0, (long long)P0 * g.n[1], T0c), b2));
+    else if (p2ok && P->tune_variant[1] != 1)
+      TRY(p2_c2c<+1>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, g.n[2], l1,
                      p2_store(P, W2, P0, (long long)P0 * g.n[1], T0c), b2));
     else
       TRY((run_fpass<T, +1, +1, false, false>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, g.n[2],
@@ -1249,6 +1252,7 @@ static pf_status gen_dctdst(pf_plan* P, const double* noise_dev, uint64_t seed, 
   nz.nsq = (unsigned)g.S;
   nz.nnoise = (unsigned)g.noise;
   nz.Dtot = (unsigned)g.D;
+  nz.transposed = g.transposed;
   const double e = sizeof(cx<T>);
   const int last = g.dim - 1;
   const long long inner = (long long)(g.N / (uint64_t)g.T[last]);

@@ -1092,6 +1092,7 @@ struct DctDstNoise {
   int ext[3];
   int D[3];
   int type;  // bit i set: axis i odd (RODFT00)
+  int transposed;  // draws in the transposed cell order (fftw.transposed): dims d-1, d-2 swapped
   const void* sq;
   const double* noise;
   uint64_t seed;
@@ -1126,7 +1127,14 @@ struct DctDstNoise {
     }
     const unsigned li = (unsigned)m[0] + (unsigned)D[0] * ((unsigned)m[1] + (unsigned)D[1] * (unsigned)m[2]);
     if (!in_bounds32(li, nsq)) return mk<T>(0, 0);
-    const unsigned ri = (unsigned)type * Dtot + li;
+    // draw order (matrix.hh:349-360): the field backend's local cells, whose last two
+    // dimensions are swapped in the transposed layout (dctdstfieldbackend.hh:855-871)
+    unsigned ci = li;
+    if (transposed && dim == 3)
+      ci = (unsigned)m[0] + (unsigned)D[0] * ((unsigned)m[2] + (unsigned)D[2] * (unsigned)m[1]);
+    else if (transposed && dim == 2)
+      ci = (unsigned)m[1] + (unsigned)D[1] * (unsigned)m[0];
+    const unsigned ri = (unsigned)type * Dtot + ci;
     T r;
     if (noise) {
       if (!in_bounds32(ri, nnoise)) return mk<T>(0, 0);

@@ -17,6 +17,8 @@
 //  - bounds violations are accumulated per thread and reported by one atomic at the end.
 #pragma once
 
+#include <cuda.h>
+
 #include "pf_fastfft.cuh"
 
 namespace pf {
@@ -202,8 +204,9 @@ __device__ __forceinline__ void p2_copy_table(float4* dst, const float4* __restr
   for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
 }
 
+// bit 1: an index outside its buffer (access skipped); bit 2: a bounded wait gave up
 __device__ __forceinline__ void p2_report(unsigned bad) {
-  if (bad) atomicOr(&g_bounds_error, 1u);
+  if (bad) atomicOr(&g_bounds_error, bad);
 }
 
 // ---------------------------------------------------------------------------
@@ -588,6 +591,128 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
       if (j < Lout) st.store_t(so, j, x);
     });
   }
+  p2_report(bad);
+}
+
+// ---------------------------------------------------------------------------
+// Strided complex pass with its tiles staged by the tensor memory accelerator.  A tile
+// (NP adjacent pencils x L rows, 32 KB for every L) is one or more 2D bulk tensor copies
+// from HBM into shared memory (cp.async.bulk.tensor, completion counted on an mbarrier);
+// two tile buffers alternate over the persistent loop, so the copy of the CTA's next tile
+// runs while the current one is transformed.  No register or LSU work moves the inputs;
+// the transform and the stores are those of kp2_c2c.  Columns beyond the last pencil and
+// rows beyond the array read as zero (TMA out-of-bounds fill), rows j >= Lin of a tile are
+// zeroed on the shared-memory read.  Every mbarrier wait is bounded: a wait that gives up
+// sets bit 2 of the error word and the CTA leaves the loop (all threads together).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+constexpr uint32_t kTmaWaitLimit = 1u << 22;  // try_wait rounds before a wait gives up
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kTmaWaitLimit; i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// 2D tile copy global -> shared (no multicast), completion on `bar`
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          smem_u32(dst)),
+      "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+template <int L>
+struct P2Tma {
+  static constexpr int BOXR = L < 256 ? L : 256;              // rows per copy (box limit 256)
+  static constexpr unsigned TILE_BYTES = (unsigned)L * P2Geom<L>::NP * 8u;  // 32 KB
+  static constexpr size_t smem_bytes() {
+    return 2 * (size_t)TILE_BYTES + (size_t)(P2Geom<L>::Q * P2Geom<L>::PLQ + P2Geom<L>::NTW) * 16 + 2 * 8;
+  }
+};
+
+template <int L, int S>
+__global__ void __launch_bounds__(kP2Threads, 2)
+    kp2_c2c_tma(const __grid_constant__ CUtensorMap src, const float4* __restrict__ twg, long long ntiles, int tpo,
+                int rows_per_outer, int Lin, int Lout, P2ArrStore st) {
+  using G = P2Geom<L>;
+  using M = P2Tma<L>;
+  extern __shared__ __align__(128) float4 p2_tma_smem[];
+  float4* tb0 = p2_tma_smem;
+  float4* tb1 = p2_tma_smem + M::TILE_BYTES / 16;
+  float4* buf = p2_tma_smem + 2 * (M::TILE_BYTES / 16);
+  float4* tw = buf + G::Q * G::PLQ;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + G::NTW);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  p2_copy_table(tw, twg, G::NTW);
+  __syncthreads();
+  const int q = tid % G::Q, u = tid / G::Q;
+  unsigned bad = 0;
+  auto issue = [&](long long t, int slot) {
+    const int o = (int)(t / tpo);
+    const int p0 = (int)(t - (long long)o * tpo) * G::NP;
+    float4* dst = slot ? tb1 : tb0;
+    fence_proxy_async();  // the buffer's previous contents were read through the generic proxy
+    mbar_expect_tx(&bar[slot], M::TILE_BYTES);
+#pragma unroll
+    for (int c = 0; c < L / M::BOXR; c++)
+      tma_load_2d(dst + c * (M::BOXR * G::NP / 2), &src, &bar[slot], p0, o * rows_per_outer + c * M::BOXR);
+  };
+  long long tile = blockIdx.x;
+  if (tid == 0 && tile < ntiles) issue(tile, 0);
+  int k = 0;
+  bool pending_next = false;
+  for (; tile < ntiles; tile += gridDim.x, k++) {
+    const int slot = k & 1;
+    const long long next = tile + gridDim.x;
+    pending_next = next < ntiles;
+    // the other buffer was last read before a barrier of the previous tile's transform
+    if (tid == 0 && pending_next) issue(next, slot ^ 1);
+    const bool ok = mbar_wait_bounded(&bar[slot], (uint32_t)(k >> 1) & 1u);
+    if (!__syncthreads_and(ok)) {
+      bad |= 2u;
+      break;
+    }
+    pending_next = false;
+    const int o = (int)(tile / tpo);
+    const int p = (int)(tile - (long long)o * tpo) * G::NP + 2 * q;
+    const float4* t4 = slot ? tb1 : tb0;
+    P2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const int j = u + r * G::TP;
+      const float4 sv = j < Lin ? t4[j * (G::NP / 2) + q] : make_float4(0.f, 0.f, 0.f, 0.f);
+      v[r] = {make_float2(sv.x, sv.z), make_float2(sv.y, sv.w)};
+    }
+    const P2ArrStore::Tile so = st.tile(p, o, Lout, bad);
+    p2_transform<L, S>(v, buf, tw, u, q, [&](int j, const P2& x) {
+      if (j < Lout) st.store_t(so, j, x);
+    });
+  }
+  if ((bad & 2u) && tid == 0 && pending_next)  // a copy issued before the failed wait: bounded wait for it
+    mbar_wait_bounded(&bar[(k & 1) ^ 1], (uint32_t)((k + 1) >> 1) & 1u);
   p2_report(bad);
 }
 

@@ -288,3 +288,48 @@ def test_fp32_fused_matvec_lengths(oracle, name, op):
     out = P.matvec(x.astype(np.float32), op=op, precision=pfb200.PREC_F32)
     assert rel(out, ref) < TOL32
     P.close()
+
+
+def _force_variant(P, pass_index, variant):
+    """measured planning, then the wisdom entry of one pass replaced by `variant`"""
+    pfb200.wisdom_forget()
+    P.autotune(repetitions=1)
+    lines = pfb200.wisdom_export().strip().splitlines()
+    out = []
+    for line in lines:
+        f = line.split()
+        if int(f[0]) == pass_index:
+            f[5] = str(variant)
+        out.append(" ".join(f))
+    pfb200.wisdom_forget()
+    pfb200.wisdom_import("\n".join(out) + "\n")
+    assert P.autotune() is False  # taken from the wisdom
+
+
+@pytest.mark.parametrize("name", ["c2", "3d-exp-d1-1024", "3d-exp-d1-2048", "3d-128", "3d-256"])
+def test_tma_staged_strided_pass(oracle, name):
+    """The strided generation pass with TMA-staged tiles (tuning variant 2) gives the same
+    realizations as the oracle on the reproduced counters, for every paired length."""
+    cfgs = dict(LONG, c2=C2, **{"3d-128": dict(dim=3, cells=(48, 64, 40), covariance="exponential",
+                                                  corr_length=0.1, approximate=True),
+                                "3d-256": dict(dim=3, cells=(40, 128, 24), covariance="matern32",
+                                               corr_length=(0.1, 0.05, 0.1), anisotropy="axiparallel",
+                                               approximate=True)})
+    d = desc_of(cfgs[name], precision=pfb200.PREC_F32)
+    g = oracle.resolve(d)
+    lam, _, _ = oracle.spectrum(d)
+    P = pfb200.Plan(d)
+    P.spectrum_build()
+    _force_variant(P, 1, 2)
+    P.profile(True)
+    P.generate(seed=1)
+    assert "gen_c2c_d1_tma" in [r["name"] for r in P.profile_read()]  # the TMA kernel ran
+    P.profile(False)
+    for seed in (5, 6):
+        ref, _ = oracle.generate(d, lam, counter_noise(g, seed, False))
+        assert rel(P.generate(seed=seed), ref) < TOL32, seed
+    noise = oracle.noise(3, g.noise)
+    ref, _ = oracle.generate(d, lam, noise)
+    assert rel(P.generate(noise=noise), ref) < TOL32
+    P.close()
+    pfb200.wisdom_forget()

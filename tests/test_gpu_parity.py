@@ -478,9 +478,26 @@ def test_dctdst_matvec_parity(oracle, name, prec):
     P.close()
 
 
-def test_dctdst_rejects_transposed():
-    with pytest.raises(pfb200.PfError):
-        pfb200.Plan(desc_of(DCTDST["2d-exp-iso"], field_backend=pfb200.FIELD_DCTDST))
+@pytest.mark.parametrize("name", list(DCTDST))
+def test_dctdst_transposed_draw_order(oracle, name):
+    """The reference's default fftw.transposed (dim > 1): the draws of each symmetry type
+    follow the field backend's local cells with the last two dimensions swapped
+    (dctdstfieldbackend.hh:855-871, matrix.hh:349-360); buffered noise and seeded
+    generation against the oracle, whose eigenvalues are taken in the natural layout."""
+    d = desc_of(DCTDST[name], field_backend=pfb200.FIELD_DCTDST, matrix_backend=pfb200.MATRIX_DCT)
+    dr = desc_of(DCTDST[name], field_backend=pfb200.FIELD_R2C, matrix_backend=pfb200.MATRIX_DCT, transposed=0)
+    lam, _, _ = oracle.spectrum(dr)
+    P = pfb200.Plan(d)
+    assert P.info.transposed == 1
+    P.spectrum_build()
+    noise = oracle.noise(11, P.info.noise_size)
+    assert rel(P.generate(noise=noise), oracle.generate_dctdst(d, lam, noise)) < TOL64F
+    # the untransposed plan on the same buffer gives a different field (another draw order)
+    Pn = pfb200.Plan(desc_of(DCTDST[name], field_backend=pfb200.FIELD_DCTDST, matrix_backend=pfb200.MATRIX_DCT,
+                             transposed=0))
+    assert rel(Pn.generate(noise=noise), oracle.generate_dctdst(d, lam, noise)) > 1e-3
+    P.close()
+    Pn.close()
 
 
 @pytest.mark.parametrize("name", ["3d-matern32-axi-pow2", "2d-exp-prime"])
