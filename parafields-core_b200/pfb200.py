@@ -240,6 +240,23 @@ def _check(st):
         raise PfError(st, msg)
 
 
+def _numel(a):
+    return a.size if isinstance(a, np.ndarray) else a.numel()
+
+
+def _itemsize(a):
+    return a.itemsize if isinstance(a, np.ndarray) else a.element_size()
+
+
+def _need(a, count, itemsize, what):
+    """the library writes/reads raw pointers: refuse buffers smaller than the call needs"""
+    if a is None:
+        return
+    if _numel(a) < count or _itemsize(a) != itemsize:
+        raise ValueError(f"{what}: buffer of {_numel(a)} x {_itemsize(a)} bytes, "
+                         f"the call needs {count} x {itemsize} bytes")
+
+
 def _ptr(a):
     """(pointer, memory kind) for a numpy array or a torch CUDA tensor."""
     if a is None:
@@ -307,9 +324,14 @@ class Plan:
         p = self.info.precision if precision is None else precision
         return np.float64 if p == PREC_F64 else np.float32
 
+    def _fsize(self):
+        return 8 if self.info.precision == PREC_F64 else 4
+
     def generate(self, noise=None, seed=0, out=None, apply_transform=False):
         if out is None:
             out = np.empty(self.info.domain_size, dtype=self._field_dtype())
+        _need(out, self.info.domain_size, self._fsize(), "generate out")
+        _need(noise, self.info.noise_size, 8, "generate noise")
         nptr, nmem = _ptr(noise)
         optr, omem = _ptr(out)
         _check(lib().pf_generate(self.h, nptr, nmem, seed, optr, omem, int(apply_transform)))
@@ -318,6 +340,7 @@ class Plan:
     def generate_batch(self, seed, count, out=None, apply_transform=False):
         if out is None:
             out = np.empty(self.info.domain_size * count, dtype=self._field_dtype())
+        _need(out, self.info.domain_size * count, self._fsize(), "generate_batch out")
         optr, omem = _ptr(out)
         _check(lib().pf_generate_batch(self.h, seed, count, optr, omem, int(apply_transform)))
         return out
@@ -325,6 +348,9 @@ class Plan:
     def matvec(self, x, op=OP_MUL, precision=PREC_F64, out=None):
         if out is None:
             out = np.empty_like(x)
+        es = 8 if precision == PREC_F64 else 4
+        _need(x, self.info.domain_size, es, "matvec in")
+        _need(out, self.info.domain_size, es, "matvec out")
         iptr, mem = _ptr(x)
         optr, _ = _ptr(out)
         _check(lib().pf_matvec(self.h, op, precision, iptr, optr, mem))
@@ -334,6 +360,8 @@ class Plan:
                          inner_fp32=False, precondition=True):
         if x is None:
             x = np.empty_like(b)
+        _need(b, self.info.domain_size, 8, "multiply_inverse b")
+        _need(x, self.info.domain_size, 8, "multiply_inverse x")
         opts = CgOpts(mode, max_iterations, tolerance, int(inner_fp32), int(precondition))
         rep = CgReport()
         bptr, mem = _ptr(b)
@@ -349,6 +377,8 @@ class Plan:
         if X is None:
             X = np.empty_like(B)
         count = B.shape[0]
+        _need(B, self.info.domain_size * count, 8, "multiply_inverse_batch B")
+        _need(X, self.info.domain_size * count, 8, "multiply_inverse_batch X")
         opts = CgOpts(mode, max_iterations, tolerance, int(inner_fp32), int(precondition))
         reps = (CgReport * count)()
         bptr, mem = _ptr(B)
