@@ -283,7 +283,11 @@ pf_status pf_spectrum_copy(pf_plan* plan, double* out, uint64_t count);
 pf_status pf_generate(pf_plan* plan, const double* noise, int32_t noise_mem, uint64_t seed,
                       void* out, int32_t out_mem, int32_t apply_transform);
 
-/* `count` realizations keyed by seed, seed+1, ... written back to back into `out`. */
+/* `count` realizations keyed by seed, seed+1, ... written back to back into `out` (which must
+ * hold count * prod(cells) values).  For the R2C field backend the realizations run on two
+ * streams: alternating, or (device output, chosen by pf_plan_autotune when faster) as a
+ * stage pipeline with the noise pass of one realization beside the remaining passes of the
+ * previous one. */
 pf_status pf_generate_batch(pf_plan* plan, uint64_t seed, int32_t count, void* out,
                             int32_t out_mem, int32_t apply_transform);
 
@@ -406,7 +410,9 @@ pf_status pf_plan_set_preconditioner(pf_plan* plan, pf_learned* learned);
  * takes them without timing (*timed = 0).  Clears the plan's profiling records.  R2C field
  * backend only (other plans: no-op). */
 pf_status pf_plan_autotune(pf_plan* plan, int32_t repetitions, int32_t* timed);
-/* Wisdom as text, one line "pass L pencils outer precision variant ctas_per_sm" per entry;
+/* Wisdom as text, one line "pass L pencils outer precision variant ctas_per_sm" per entry
+ * (pass 0..2 the realization passes; pass 3 holds the batch mode of pf_generate_batch:
+ * variant 0 realizations alternating over two streams, 1 the stage pipeline);
  * *needed = bytes including the terminating NUL. */
 pf_status pf_wisdom_export(char* buf, uint64_t cap, uint64_t* needed);
 pf_status pf_wisdom_import(const char* text);

@@ -254,6 +254,10 @@ struct pf_plan {
   // factor arrays (shared = true: it frees only its own workspaces, scratch and stream)
   bool shared = false;
   std::vector<pf_plan*> lanes;
+  // pf_generate_batch to device memory: 0 = realizations alternate over two streams,
+  // 1 = stage pipeline (noise passes on one stream, the remaining passes on the other)
+  int batch_mode = 0;
+  cudaEvent_t stage_ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 static pf_status dalloc(pf_plan* P, void** p, size_t bytes) {
@@ -1089,8 +1093,10 @@ static pf_status factor_array(pf_plan* P, int op, const T** out) {
 // ---------------------------------------------------------------------------
 // generation: generateField (matrix.hh:330-421)
 // ---------------------------------------------------------------------------
+// stages: bit 0 the noise pass (noise, scaling, backward transform along the last axis into
+// workspace 0), bit 1 the remaining passes (workspace 0 -> field); both for one realization
 template <typename T, typename S>
-static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* out, int transform) {
+static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* out, int transform, int stages = 3) {
   const Geom& g = P->g;
   const int T0c = g.T0c, P0 = half_pitch(g);
   R2CNoise nz{};
@@ -1133,7 +1139,8 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
     ~CapReset() { P->grid_cap = 0; }
   } cap_reset{P};
   P->grid_cap = P->tune_grid[0];
-  if (F32 && P->tune_variant[0] == 0 && p2_length(Tl) && p2_view_ok(W1, jst, P0, outer))
+  if (!(stages & 1)) {
+  } else if (F32 && P->tune_variant[0] == 0 && p2_length(Tl) && p2_view_ok(W1, jst, P0, outer))
     TRY(p2_noise(P, "gen_noise_last", Tl, g.n[last], T0c, outer, nz, p2_store(P, W1, jst, P0, T0c), b1));
   else if (Tl % 2 == 0)
     TRY((run_fpass<T, +1, +1, false, true>(P, "gen_noise_last", Tl, g.n[last], T0c, outer, nz, NoMid(),
@@ -1141,6 +1148,7 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
   else
     TRY((run_fpass<T, +1, +1, false, false>(P, "gen_noise_last", Tl, g.n[last], T0c, outer, nz, NoMid(),
                                             arr_store<cx<T>>(P, W1, jst, P0, 1), b1)));
+  if (!(stages & 2)) return PF_OK;
   void* cur = W1;
   if (g.dim == 3) {
     void* W2 = nullptr;
@@ -1469,6 +1477,65 @@ static pf_status generate_typed(pf_plan* P, const double* nd, uint64_t seed, S* 
   return PF_OK;
 }
 
+// Stage pipeline of pf_generate_batch (device output, R2C field backend): the noise pass of
+// realization r (issue-bound: integer multiplies and paired FP32 arithmetic) runs on one
+// stream while the memory-bound remaining passes of realization r-1 run on the other.  The
+// noise passes alternate between two intermediate buffers; events order every buffer's
+// reuse after the passes that read it.
+static pf_status generate_stage_pipeline(pf_plan* P, uint64_t seed, int32_t count, void* out, int tr) {
+  if (!P->lane[0])
+    for (int l = 0; l < 2; l++) CK(cudaStreamCreateWithFlags(&P->lane[l], cudaStreamNonBlocking));
+  if (!P->lane_ev[0])
+    for (int l = 0; l < 3; l++) CK(cudaEventCreateWithFlags(&P->lane_ev[l], cudaEventDisableTiming));
+  if (!P->stage_ev[0])
+    for (int l = 0; l < 4; l++) CK(cudaEventCreateWithFlags(&P->stage_ev[l], cudaEventDisableTiming));
+  const bool f64 = P->desc.precision == PF_PREC_F64;
+  const size_t bytes = P->g.domain * (f64 ? 8 : 4);
+  cudaStream_t caller = P->stream;
+  CK(cudaEventRecord(P->lane_ev[0], caller));
+  for (int l = 0; l < 2; l++) CK(cudaStreamWaitEvent(P->lane[l], P->lane_ev[0], 0));
+  cudaEvent_t* noise_done = P->stage_ev;      // [slot]: the noise pass wrote the buffer
+  cudaEvent_t* buffer_free = P->stage_ev + 2;  // [slot]: the remaining passes read it
+  pf_status st = PF_OK;
+  for (int32_t r = 0; r < count && st == PF_OK; r++) {
+    const int slot = r & 1;
+    auto run = [&](int stages) {
+      if (slot) {
+        std::swap(P->ws[0], P->ws_b[0]);
+        std::swap(P->ws_bytes[0], P->ws_b_bytes[0]);
+      }
+      void* dst = (char*)out + (size_t)r * bytes;
+      const pf_status s2 = f64 ? gen_r2c<double, double>(P, nullptr, seed + r, (double*)dst, tr, stages)
+                               : gen_r2c<float, float>(P, nullptr, seed + r, (float*)dst, tr, stages);
+      if (slot) {
+        std::swap(P->ws[0], P->ws_b[0]);
+        std::swap(P->ws_bytes[0], P->ws_b_bytes[0]);
+      }
+      return s2;
+    };
+    P->stream = P->lane[0];
+    if (r >= 2 && cudaStreamWaitEvent(P->lane[0], buffer_free[slot], 0) != cudaSuccess)
+      st = fail(PF_ERR_CUDA, "stream wait failed");
+    if (st == PF_OK) st = run(1);
+    if (st == PF_OK && cudaEventRecord(noise_done[slot], P->lane[0]) != cudaSuccess)
+      st = fail(PF_ERR_CUDA, "event record failed");
+    P->stream = P->lane[1];
+    if (st == PF_OK && cudaStreamWaitEvent(P->lane[1], noise_done[slot], 0) != cudaSuccess)
+      st = fail(PF_ERR_CUDA, "stream wait failed");
+    if (st == PF_OK) st = run(2);
+    if (st == PF_OK && cudaEventRecord(buffer_free[slot], P->lane[1]) != cudaSuccess)
+      st = fail(PF_ERR_CUDA, "event record failed");
+    P->stream = caller;
+  }
+  P->stream = caller;
+  for (int l = 0; l < 2; l++) {
+    CK(cudaEventRecord(P->lane_ev[1 + l], P->lane[l]));
+    CK(cudaStreamWaitEvent(caller, P->lane_ev[1 + l], 0));
+  }
+  P->spare_valid = false;
+  return st;
+}
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -1570,6 +1637,8 @@ void pf_plan_destroy(pf_plan* P) {
   }
   for (int l = 0; l < 3; l++)
     if (P->lane_ev[l]) cudaEventDestroy(P->lane_ev[l]);
+  for (int l = 0; l < 4; l++)
+    if (P->stage_ev[l]) cudaEventDestroy(P->stage_ev[l]);
   if (P->own) cudaStreamDestroy(P->own);
   delete P;
 }
@@ -1697,6 +1766,8 @@ pf_status pf_generate_batch(pf_plan* P, uint64_t seed, int32_t count, void* out,
   const size_t es = P->desc.precision == PF_PREC_F64 ? 8 : 4;
   const size_t bytes = P->g.domain * es;
   const int tr = apply_transform ? P->desc.transform : 0;
+  if (P->g.fb == PF_FIELD_R2C && count >= 2 && P->batch_mode == 1 && out_mem == PF_MEM_DEVICE)
+    return check_bounds(P, generate_stage_pipeline(P, seed, count, out, tr));
   if (P->g.fb == PF_FIELD_R2C && count >= 2) {
     // Realizations are independent: alternate them over two streams, each with its own
     // workspaces, so that one realization's issue-bound noise pass overlaps the other's

@@ -500,12 +500,26 @@ def test_dctdst_transposed_draw_order(oracle, name):
     Pn.close()
 
 
+@pytest.mark.parametrize("mode", [0, 1])
 @pytest.mark.parametrize("name", ["3d-matern32-axi-pow2", "2d-exp-prime"])
-def test_pipelined_batch_equals_single_calls(name):
+def test_pipelined_batch_equals_single_calls(name, mode):
     """pf_generate_batch with device output alternates realizations over two streams with
     separate workspaces; every realization equals the one-at-a-time call with its seed."""
     torch = pytest.importorskip("torch")
-    P = pfb200.Plan(desc_of(CONFIGS[name], precision=pfb200.PREC_F32))
+    d = desc_of(CONFIGS[name], precision=pfb200.PREC_F32)
+    P = pfb200.Plan(d)
+    pfb200.wisdom_forget()
+    P.autotune(repetitions=1)
+    lines = [l.split() for l in pfb200.wisdom_export().strip().splitlines()]
+    for f in lines:
+        if f[0] == "3":
+            f[5] = str(mode)
+    pfb200.wisdom_forget()
+    pfb200.wisdom_import("\n".join(" ".join(f) for f in lines) + "\n")
+    P.close()
+    P = pfb200.Plan(d)
+    assert P.autotune() is False  # choices and batch mode from the wisdom
+    pfb200.wisdom_forget()
     n = P.info.domain_size
     batch = torch.empty(5 * n, dtype=torch.float32, device="cuda")
     P.generate_batch(seed=41, count=5, out=batch)
@@ -529,7 +543,7 @@ def test_autotune_and_wisdom(oracle, name):
     assert P.autotune(repetitions=2) is True
     assert rel(P.generate(noise=noise), ref) < TOL32
     text = pfb200.wisdom_export()
-    assert len(text.strip().splitlines()) == g.dim
+    assert len(text.strip().splitlines()) == g.dim + 1  # the passes and the batch mode
     P2 = pfb200.Plan(d)
     assert P2.autotune() is False
     pfb200.wisdom_forget()
