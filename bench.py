@@ -180,6 +180,15 @@ def cpu_oracle_realization(threads):
     return time.perf_counter() - t0, g.domain, noise, field, lam
 
 
+def cpu_oracle_field(noise, lam, desc_kw=WORKLOAD):
+    """the oracle's FP64 realization of a workload from a given noise buffer"""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import pfb200
+    field, _ = O.generate(pfb200.make_desc(**desc_kw), lam, noise)
+    return field
+
+
 def cpu_scipy_realization(threads, lam, noise, cells=WORKLOAD["cells"]):
     """The same realization with scipy.fft (pocketfft, `workers` threads) for the transform:
     eigenvalue-scaled half spectrum (the oracle's noise and eigenvalues, R2C layout with the
@@ -363,11 +372,20 @@ def run_b200(args):
             P.generate(noise=hn, out=out)
             torch.cuda.synchronize()
             gf = out.double().cpu().numpy()
+            # the first realization of the timed batch itself (seeded on-device noise): its
+            # noise exported in the reference draw order and fed to the oracle
+            tnoise = P.export_noise(seed0 + 100)
+            tfield = cpu_oracle_field(tnoise, lam)
+            tf = outs[:n].double().cpu().numpy()
             err = {"rel_l2_error_vs_oracle": float(np.linalg.norm(gf - ofield) / np.linalg.norm(ofield)),
                    "max_abs_error_vs_oracle": float(np.abs(gf - ofield).max()),
+                   "timed_realization_rel_l2_error_vs_oracle":
+                       float(np.linalg.norm(tf - tfield) / np.linalg.norm(tfield)),
                    "note": "one FP32 realization of the timed workload fed the oracle's N(0,1) buffer "
                            "(seed 20261203, reference draw order), against the FP64 oracle on the same "
-                           "buffer; tolerance of the parity tests 1e-5"}
+                           "buffer; and the first realization of the timed batch (seeded on-device noise, "
+                           "exported with pf_export_noise) against the oracle fed that noise; tolerance "
+                           "of the parity tests 1e-5"}
             del hn
         clocks = clk.summary()
         line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
@@ -454,6 +472,33 @@ def c3_descs(count, precision, seed=20261203):
     return out
 
 
+def ensemble_oracle_sample(E, descs, out, seed, epoch, count=6):
+    """CPU baseline leg of the ensemble workload: the FP64 oracle on a sample of fields, fed
+    each field's exported noise (seed + i, the ensemble call `epoch`), timed and used as the
+    checker of the GPU fields of that call"""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import pfb200
+    O.set_threads(os.cpu_count() or 1)
+    idx = sorted(set(int(i) for i in np.linspace(0, len(descs) - 1, count)))
+    errs, cells, secs = [], 0, 0.0
+    for i in idx:
+        d = descs[i]
+        P = pfb200.Plan(d)
+        noise = P.export_noise(seed + i, epoch)
+        P.close()
+        lam, _, _ = O.spectrum(d)
+        t0 = time.perf_counter()
+        ref, _ = O.generate(d, lam, noise)
+        secs += time.perf_counter() - t0
+        cells += ref.size
+        f = out[int(E.offsets[i]):int(E.offsets[i + 1])].double().cpu().numpy()
+        errs.append(float(np.linalg.norm(f - ref) / np.linalg.norm(ref)))
+    return ({"fields": idx, "rel_l2": errs, "max": max(errs)},
+            {"value": cells / secs, "unit": "cells/s", "cores": os.cpu_count(), "kind": "port",
+             "sample": f"{len(idx)} fields of the ensemble, one FP64 realization each by the oracle"})
+
+
 def run_ensemble(args):
     """Uneven 2D fields: mixed (FP32 realizations, FP64 spectra) graph replay vs FP64 replay
     vs the plain FP64 path (one plan and one pf_generate per field, every field)."""
@@ -483,7 +528,11 @@ def run_ensemble(args):
         e1.record(s)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
+        errs, cpu = None, None
+        if prec == pfb200.PREC_F32 and not args.no_cpu_baseline:
+            errs, cpu = ensemble_oracle_sample(E, descs, out, seed=1, epoch=1)
         res[name] = {"cells": E.total, "ms_per_ensemble": ms, "cells_per_s": E.total / (ms / 1e3),
+                     "error_vs_oracle_sample": errs, "cpu_baseline_sample": cpu,
                      "spectra_s": tspec, "autotune_s": ttune, "fields_timed_by_autotune": timed,
                      "fields_with_negative_eigenvalues": sum(1 for x in st if x["negative"]),
                      "launches_per_replay": E.launches_per_replay()}

@@ -283,6 +283,15 @@ pf_status pf_spectrum_copy(pf_plan* plan, double* out, uint64_t count);
 pf_status pf_generate(pf_plan* plan, const double* noise, int32_t noise_mem, uint64_t seed,
                       void* out, int32_t out_mem, int32_t apply_transform);
 
+/* The noise a seeded pf_generate call of this plan draws (seed, and the epoch an ensemble
+ * mixes in: 0 for plans, the call number for ensemble fields), written as info.noise_size
+ * doubles in the reference's draw order (rand1, rand2 per stored frequency,
+ * matrix.hh:378-404) into `out` (memory `mem`).  Fed to pf_generate as a noise buffer, or to
+ * a host implementation of the reference, it reproduces the seeded realization (to the
+ * rounding of the plan's precision).  No counterpart in the reference, whose noise comes from
+ * host generators.  R2C field backend only (PF_ERR_CONFIG otherwise). */
+pf_status pf_export_noise(pf_plan* plan, uint64_t seed, uint32_t epoch, double* out, int32_t mem);
+
 /* `count` realizations keyed by seed, seed+1, ... written back to back into `out` (which must
  * hold count * prod(cells) values).  For the R2C field backend the realizations run on two
  * streams: alternating, or (device output, chosen by pf_plan_autotune when faster) as a

@@ -1918,6 +1918,33 @@ pf_status pf_multiply_inverse_batch(pf_plan* P, const double* B, double* X, int3
   return check_bounds(P, cg_solve_batch(P, B, X, count, mem, o, reports, lanes));
 }
 
+pf_status pf_export_noise(pf_plan* P, uint64_t seed, uint32_t epoch, double* out, int32_t mem) {
+  if (!P || !out) return fail(PF_ERR_ARG, "null argument");
+  const Geom& g = P->g;
+  if (g.fb != PF_FIELD_R2C) return fail(PF_ERR_CONFIG, "noise export serves the R2C field backend");
+  NoiseExport e{};
+  e.dim = g.dim;
+  e.T0c = g.T0c;
+  e.ext1 = g.T[1];
+  e.ext2 = g.T[2];
+  e.Tl = g.T[g.dim - 1];
+  e.transposed = g.transposed;
+  e.fp64 = P->desc.precision == PF_PREC_F64;
+  e.seed = seed;
+  e.epoch = epoch;
+  e.n = g.noise;
+  double* dst = out;
+  if (mem != PF_MEM_DEVICE) {
+    TRY(ensure(P, (void**)&P->noise_dev, &P->noise_cap, g.noise * 8));
+    dst = P->noise_dev;
+  }
+  k_export_noise<<<grid_for(g.Nc), kThreads, 0, P->stream>>>(e, dst);
+  P->launches++;
+  CK(cudaGetLastError());
+  if (mem != PF_MEM_DEVICE) CK(cudaMemcpyAsync(out, dst, g.noise * 8, cudaMemcpyDeviceToHost, P->stream));
+  return check_bounds(P, PF_OK);
+}
+
 pf_status pf_apply_transform(pf_plan* P, int32_t precision, void* data, uint64_t count, int32_t mem) {
   if (!P || !data) return fail(PF_ERR_ARG, "null argument");
   const size_t es = precision == PF_PREC_F64 ? 8 : 4;

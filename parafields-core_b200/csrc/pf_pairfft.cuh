@@ -364,6 +364,71 @@ __device__ __forceinline__ P2 box_muller_pair(uint32_t a, uint32_t b, uint32_t c
   return {f2mul(rad, make_float2(cA, cB)), f2mul(rad, make_float2(sA, sB))};
 }
 
+// The seeded noise of the R2C field backend written out in the reference's draw order
+// (rand1, rand2 per stored frequency): the same counters, Philox4x32-10 words and
+// Box-Muller definitions as the generation passes (paired FP32 form for FP32 plans, the FP64
+// form for FP64 plans), so that a host implementation fed these values reproduces a seeded
+// realization.  One thread per stored frequency k (last-axis index kl < T/2 when the last
+// extent is even: it also writes the partner kl + T/2 from the same counter).
+struct NoiseExport {
+  int dim, T0c, ext1, ext2, Tl;
+  int transposed, fp64;
+  uint64_t seed;
+  uint32_t epoch;
+  unsigned long long n;  // doubles in `out`
+  __device__ __forceinline__ unsigned stored(int k0, int k1, int kl) const {
+    if (dim == 2) return (unsigned)k0 + (unsigned)T0c * (unsigned)kl;
+    if (transposed) return (unsigned)k0 + (unsigned)T0c * ((unsigned)kl + (unsigned)ext2 * (unsigned)k1);
+    return (unsigned)k0 + (unsigned)T0c * ((unsigned)k1 + (unsigned)ext1 * (unsigned)kl);
+  }
+};
+
+__global__ void k_export_noise(NoiseExport e, double* __restrict__ out) {
+  const bool paired = e.Tl % 2 == 0;
+  const int kls = paired ? e.Tl / 2 : e.Tl;
+  const int n1 = e.dim == 3 ? e.ext1 : 1;
+  const long long total = (long long)e.T0c * n1 * kls;
+  const uint2 key = make_uint2((uint32_t)e.seed, (uint32_t)(e.seed >> 32));
+  unsigned bad = 0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int k0 = (int)(t % e.T0c);
+    const long long rest = t / e.T0c;
+    const int k1 = (int)(rest % n1);
+    const int kl = (int)(rest / n1);
+    const unsigned s0 = e.stored(k0, k1, kl);
+    const uint4 c = philox4x32_10(pair_counter(s0, e.epoch), key);
+    double r[4];
+    if (e.fp64) {
+      box_muller(c.x, c.y, r[0], r[1]);
+      box_muller(c.z, c.w, r[2], r[3]);
+    } else {
+      const float2 a = box_muller_fast(c.x, c.y), b = box_muller_fast(c.z, c.w);
+      r[0] = a.x;
+      r[1] = a.y;
+      r[2] = b.x;
+      r[3] = b.y;
+    }
+    const unsigned long long i0 = 2ull * s0;
+    if (i0 + 1 < e.n) {
+      out[i0] = r[0];
+      out[i0 + 1] = r[1];
+    } else {
+      bad = 1;
+    }
+    if (paired) {
+      const unsigned long long i1 = 2ull * e.stored(k0, k1, kl + kls);
+      if (i1 + 1 < e.n) {
+        out[i1] = r[2];
+        out[i1 + 1] = r[3];
+      } else {
+        bad = 1;
+      }
+    }
+  }
+  if (bad) atomicOr(&g_bounds_error, 1u);
+}
+
 template <int DIM, int LAYOUT, bool TRANSP>
 struct P2Noise {
   // LAYOUT: 1 = DCT prod(T/2+1) eigenvalues (mirrored lookup), 0 = R2C half spectrum,

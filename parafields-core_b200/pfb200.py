@@ -177,6 +177,7 @@ def lib():
         "pf_spectrum_build_values": (i32, [vp, vp, u64, i32, C.POINTER(EigStats)]),
         "pf_generate": (i32, [vp, vp, i32, u64, vp, i32, i32]),
         "pf_generate_batch": (i32, [vp, u64, i32, vp, i32, i32]),
+        "pf_export_noise": (i32, [vp, u64, C.c_uint32, vp, i32]),
         "pf_matvec": (i32, [vp, i32, i32, vp, vp, i32]),
         "pf_matvec_static": (i32, [vp, i32, vp, vp]),
         "pf_multiply_inverse": (i32, [vp, vp, vp, i32, C.POINTER(CgOpts), C.POINTER(CgReport)]),
@@ -335,6 +336,15 @@ class Plan:
         nptr, nmem = _ptr(noise)
         optr, omem = _ptr(out)
         _check(lib().pf_generate(self.h, nptr, nmem, seed, optr, omem, int(apply_transform)))
+        return out
+
+    def export_noise(self, seed, epoch=0, out=None):
+        """the noise of a seeded realization in the reference's draw order (doubles)"""
+        if out is None:
+            out = np.empty(self.info.noise_size, dtype=np.float64)
+        _need(out, self.info.noise_size, 8, "export_noise out")
+        ptr, mem = _ptr(out)
+        _check(lib().pf_export_noise(self.h, seed, epoch, ptr, mem))
         return out
 
     def generate_batch(self, seed, count, out=None, apply_transform=False):

@@ -333,3 +333,45 @@ def test_tma_staged_strided_pass(oracle, name):
     assert rel(P.generate(noise=noise), ref) < TOL32
     P.close()
     pfb200.wisdom_forget()
+
+
+@pytest.mark.parametrize("name,prec", [("c2", pfb200.PREC_F32), ("2d-exp-1024", pfb200.PREC_F32),
+                                       ("2d-exp-1024", pfb200.PREC_F64), ("3d-exp-d1-1024", pfb200.PREC_F64)])
+def test_exported_noise_reproduces_seeded_realizations(oracle, name, prec):
+    """pf_export_noise writes the seeded noise in the reference's draw order: it equals the
+    host reproduction of the counters, and the oracle fed it reproduces the seeded
+    realization (the error of a timed, seeded realization can be stated this way)."""
+    cfg = C2 if name == "c2" else LONG[name]
+    d = desc_of(cfg, precision=prec)
+    g = oracle.resolve(d)
+    lam, _, _ = oracle.spectrum(d)
+    P = pfb200.Plan(d)
+    P.spectrum_build()
+    seed, epoch = 0xC0FFEE + 3, 5 if name != "c2" else 0
+    noise = P.export_noise(seed, epoch)
+    host = counter_noise(g, seed, prec == pfb200.PREC_F64, epoch=epoch)
+    assert rel(noise, host) < (1e-12 if prec == pfb200.PREC_F64 else 1e-6)
+    ref, _ = oracle.generate(d, lam, noise)
+    if epoch == 0:
+        assert rel(P.generate(seed=seed), ref) < (1e-9 if prec == pfb200.PREC_F64 else TOL32)
+    assert rel(P.generate(noise=noise), ref) < (TOL64F if prec == pfb200.PREC_F64 else TOL32)
+    P.close()
+
+
+def test_exported_noise_states_ensemble_field_errors(oracle):
+    """Every field of an ensemble replay against the oracle fed that field's exported noise
+    (seed + i, epoch = call number)."""
+    cfgs = [LONG["2d-exp-1024"], dict(dim=2, cells=(300, 170), covariance="gaussian",
+                                       corr_length=(0.05, 0.01, -0.01, 0.04), anisotropy="geometric",
+                                       approximate=True)]
+    descs = [desc_of(c, precision=pfb200.PREC_F32) for c in cfgs]
+    E = pfb200.Ensemble(descs, seed=41)
+    E.spectra()
+    out = E.generate()  # call 1
+    for i, d in enumerate(descs):
+        P = pfb200.Plan(d)
+        lam, _, _ = oracle.spectrum(d)
+        ref, _ = oracle.generate(d, lam, P.export_noise(41 + i, 1))
+        assert rel(E.field(out, i), ref) < TOL32, i
+        P.close()
+    E.close()
