@@ -414,15 +414,19 @@ pf_status pf_plan_set_preconditioner(pf_plan* plan, pf_learned* learned);
 /* Measured planning, the counterpart of fftw.measure / fftw.useWisdom (r2cfieldbackend.hh:
  * 212-230, fieldtraits.hh:175-186): times every candidate of each realization pass of the
  * plan (paired-FP32 or scalar kernels x resident CTAs per SM of the persistent kernels,
- * `repetitions` realizations each, default 3) and keeps the fastest per pass.  Choices go to
+ * `repetitions` realizations each, default 3) and keeps the fastest per pass; then, on
+ * batches of 4 realizations, the plane groups of the last two 3D passes and the batch mode
+ * of pf_generate_batch.  Choices go to
  * a process-wide wisdom table keyed by the pass geometry; a plan whose passes are all in it
  * takes them without timing (*timed = 0).  Clears the plan's profiling records.  R2C field
  * backend only (other plans: no-op). */
 pf_status pf_plan_autotune(pf_plan* plan, int32_t repetitions, int32_t* timed);
 /* Wisdom as text, one line "pass L pencils outer precision variant ctas_per_sm" per entry
- * (pass 0..2 the realization passes; pass 3 holds the batch mode of pf_generate_batch:
- * variant 0 realizations alternating over two streams, 1 the stage pipeline);
- * *needed = bytes including the terminating NUL. */
+ * (pass 0..2 the realization passes; pass 3 holds the batch mode of pf_generate_batch in
+ * `variant` -- 0 realizations alternating over two streams, 1 the stage pipeline -- and, for
+ * 3D plans, in `ctas_per_sm` the number of plane groups over which the last two passes run
+ * in turn, each group's intermediate reusing one buffer that stays in L2; 0 or 1 = one
+ * group); *needed = bytes including the terminating NUL. */
 pf_status pf_wisdom_export(char* buf, uint64_t cap, uint64_t* needed);
 pf_status pf_wisdom_import(const char* text);
 void pf_wisdom_forget(void);

@@ -258,6 +258,10 @@ struct pf_plan {
   // 1 = stage pipeline (noise passes on one stream, the remaining passes on the other)
   int batch_mode = 0;
   cudaEvent_t stage_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // 3D generation: the middle and the complex-to-real passes run over this many groups of
+  // output planes in turn, so that the intermediate between them (one group, held in a
+  // buffer reused by every group) stays in L2 instead of crossing HBM twice; 1 = one group
+  int gen_chunks = 1;
 };
 
 static pf_status dalloc(pf_plan* P, void** p, size_t bytes) {
@@ -542,10 +546,13 @@ static pf_status run_real_pass(pf_plan* P, const char* name, int T0, int Lout, l
   return prof_end(P, &rec);
 }
 
-// capacity (bytes) of the workspace holding p: the bound every access is checked against
+// bytes from p to the end of the workspace holding it: the bound every access is checked
+// against (0 for a pointer outside the workspaces)
 static size_t cap_of(const pf_plan* P, const void* p) {
-  for (int i = 0; i < 3; i++)
-    if (p == P->ws[i]) return P->ws_bytes[i];
+  for (int i = 0; i < 3; i++) {
+    const char* b = (const char*)P->ws[i];
+    if (b && (const char*)p >= b && (const char*)p < b + P->ws_bytes[i]) return P->ws_bytes[i] - ((const char*)p - b);
+  }
   return 0;
 }
 
@@ -1114,7 +1121,6 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
   nz.nsq = (long long)g.S;
   nz.nnoise = (long long)g.noise;
   nz.Tl = g.T[g.dim - 1];
-  FieldRowStore<S> fs{out, g.n[0], transform, P->desc.boxcox_lambda, (unsigned)g.domain};
   const double e = sizeof(cx<T>);
   const double noise_b = noise_dev ? 16.0 : 0.0;
   const double lam_b = sizeof(T);
@@ -1149,52 +1155,64 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
     TRY((run_fpass<T, +1, +1, false, false>(P, "gen_noise_last", Tl, g.n[last], T0c, outer, nz, NoMid(),
                                             arr_store<cx<T>>(P, W1, jst, P0, 1), b1)));
   if (!(stages & 2)) return PF_OK;
-  void* cur = W1;
-  if (g.dim == 3) {
-    void* W2 = nullptr;
-    TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)P0 * g.n[1] * g.n[2], &W2));
-    const double b2 = (double)T0c * g.n[2] * (g.T[1] + g.n[1]) * e;
-    P->grid_cap = P->tune_grid[1];
-    const bool p2ok = F32 && p2_length(g.T[1]) && p2_view_ok(W1, P0, (long long)P0 * g.T[1], g.n[2]) &&
-                      p2_view_ok(W2, P0, (long long)P0 * g.n[1], g.n[2]);
-    const P2ArrLoad l1 = p2_load(P, W1, P0, (long long)P0 * g.T[1], g.T[1], T0c);
-    if (p2ok && P->tune_variant[1] == 2 && p2_tma_ok(P, l1, g.n[2]))  // tiles staged by TMA
-      TRY(p2_c2c_tma<+1>(P, "gen_c2c_d1_tma", g.T[1], g.n[1], T0c, g.n[2], l1,
-                         p2_store(P, W2, P0, (long long)P0 * g.n[1], T0c), b2));
-    else if (p2ok && P->tune_variant[1] != 1)
-      TRY(p2_c2c<+1>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, g.n[2], l1,
-                     p2_store(P, W2, P0, (long long)P0 * g.n[1], T0c), b2));
-    else
-      TRY((run_fpass<T, +1, +1, false, false>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, g.n[2],
-                                              arr_load<cx<T>>(P, W1, P0, (long long)P0 * g.T[1], 1, g.T[1]),
-                                              NoMid(), arr_store<cx<T>>(P, W2, P0, (long long)P0 * g.n[1], 1),
-                                              b2)));
-    cur = W2;
-  }
-  const long long rows = g.dim == 3 ? (long long)g.n[1] * g.n[2] : g.n[1];
-  const double b3 = (double)rows * (T0c * e + g.n[0] * sizeof(S));
-  P->grid_cap = P->tune_grid[2];
-  if constexpr (F32) {
-    if (P->tune_variant[2] == 0 && g.T[0] % 2 == 0 && p2_length(g.T[0] / 2)) {
-      P2RowLoad rl;
-      rl.ptr = (const float2*)cur;
-      rl.rowstride = (unsigned)P0;
-      rl.n = (unsigned)std::min<size_t>(cap_of(P, cur) / sizeof(float2), 0xffffffffu);
-      rl.Lin = T0c;
-      rl.np = (int)rows;
-      P2FieldStore ps;
-      ps.out = (float*)out;
-      ps.n0 = g.n[0];
-      ps.transform = transform;
-      ps.boxcox = (float)P->desc.boxcox_lambda;
-      ps.n = (unsigned)g.domain;
-      ps.np = (int)rows;
-      ps.Lout = g.n[0];
-      ps.vec = (g.n[0] % 2 == 0 && ((uintptr_t)out & 7u) == 0) ? 1 : 0;
-      return p2_c2r(P, "gen_c2r_d0", g.T[0] / 2, g.n[0], rows, rl, ps, b3);
+  // the complex-to-real rows of `nrows` (pencil index j1 + n1 * plane) from `src` into
+  // the field rows starting at `dst`
+  auto c2r_rows = [&](const void* src, S* dst, long long nrows) -> pf_status {
+    const double b3 = (double)nrows * (T0c * e + g.n[0] * sizeof(S));
+    P->grid_cap = P->tune_grid[2];
+    const size_t left = (size_t)(g.domain - (size_t)(dst - out));
+    if constexpr (F32) {
+      if (P->tune_variant[2] == 0 && g.T[0] % 2 == 0 && p2_length(g.T[0] / 2)) {
+        P2RowLoad rl;
+        rl.ptr = (const float2*)src;
+        rl.rowstride = (unsigned)P0;
+        rl.n = (unsigned)std::min<size_t>(cap_of(P, src) / sizeof(float2), 0xffffffffu);
+        rl.Lin = T0c;
+        rl.np = (int)nrows;
+        P2FieldStore ps;
+        ps.out = (float*)dst;
+        ps.n0 = g.n[0];
+        ps.transform = transform;
+        ps.boxcox = (float)P->desc.boxcox_lambda;
+        ps.n = (unsigned)left;
+        ps.np = (int)nrows;
+        ps.Lout = g.n[0];
+        ps.vec = (g.n[0] % 2 == 0 && ((uintptr_t)dst & 7u) == 0) ? 1 : 0;
+        return p2_c2r(P, "gen_c2r_d0", g.T[0] / 2, g.n[0], nrows, rl, ps, b3);
+      }
     }
+    FieldRowStore<S> fr{dst, g.n[0], transform, P->desc.boxcox_lambda, (unsigned)left};
+    return run_freal<T, false>(P, "gen_c2r_d0", g.T[0], g.n[0], nrows,
+                               arr_load<cx<T>>(P, src, 1, 0, P0, T0c), fr, b3);
+  };
+  if (g.dim == 2) return c2r_rows(W1, out, g.n[1]);
+  // 3D: the middle pass (along axis 1, output pruned to n1) and the complex-to-real rows
+  // run over groups of output planes (axis-2 index) in turn; the middle pass's output for
+  // one group lives in workspace 1, which every group reuses (small groups keep it in L2)
+  const int n2 = g.n[2];
+  const int groups = std::max(1, std::min(P->gen_chunks, n2));
+  const int gp = (n2 + groups - 1) / groups;  // planes per group
+  void* W2 = nullptr;
+  TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)P0 * g.n[1] * gp, &W2));
+  const long long w1_plane = (long long)P0 * g.T[1], w2_plane = (long long)P0 * g.n[1];
+  for (int z0 = 0; z0 < n2; z0 += gp) {
+    const int nz = std::min(gp, n2 - z0);
+    void* src = (char*)W1 + sizeof(cx<T>) * (size_t)w1_plane * z0;
+    const double b2 = (double)T0c * nz * (g.T[1] + g.n[1]) * e;
+    P->grid_cap = P->tune_grid[1];
+    const bool p2ok = F32 && p2_length(g.T[1]) && p2_view_ok(src, P0, w1_plane, nz) && p2_view_ok(W2, P0, w2_plane, nz);
+    const P2ArrLoad l1 = p2_load(P, src, P0, w1_plane, g.T[1], T0c);
+    if (p2ok && P->tune_variant[1] == 2 && p2_tma_ok(P, l1, nz))  // tiles staged by TMA
+      TRY(p2_c2c_tma<+1>(P, "gen_c2c_d1_tma", g.T[1], g.n[1], T0c, nz, l1, p2_store(P, W2, P0, w2_plane, T0c), b2));
+    else if (p2ok && P->tune_variant[1] != 1)
+      TRY(p2_c2c<+1>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, nz, l1, p2_store(P, W2, P0, w2_plane, T0c), b2));
+    else
+      TRY((run_fpass<T, +1, +1, false, false>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, nz,
+                                              arr_load<cx<T>>(P, src, P0, w1_plane, 1, g.T[1]), NoMid(),
+                                              arr_store<cx<T>>(P, W2, P0, w2_plane, 1), b2)));
+    TRY(c2r_rows(W2, out + (size_t)g.n[0] * g.n[1] * z0, (long long)g.n[1] * nz));
   }
-  return run_freal<T, false>(P, "gen_c2r_d0", g.T[0], g.n[0], rows, arr_load<cx<T>>(P, cur, 1, 0, P0, T0c), fs, b3);
+  return PF_OK;
 }
 
 // DFT field backend: complex noise on the whole torus, backward c2c on every axis,

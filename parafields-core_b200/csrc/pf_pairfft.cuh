@@ -24,15 +24,23 @@
 namespace pf {
 
 constexpr int kP2Threads = 256;
-// resident CTAs per SM the register allocation is sized for (per kernel family)
+// resident CTAs per SM the register allocation is sized for (per kernel family).  The
+// strided pass is held to 64 registers (4 CTAs per SM): alone it runs as fast as with 3,
+// and in the two-stream batch its CTAs fit beside the other stream's kernels (256^3
+// Matern-3/2 batch: 0.388 against 0.401 ms per realization).  At 64 registers the
+// complex-to-real pass spills and runs slower alone (0.088 against 0.077 ms) and in the
+// batch; the fused matvec pass spills too.  Both keep 3.
 #ifndef PF_P2_MIN_NOISE
 #define PF_P2_MIN_NOISE 4
 #endif
 #ifndef PF_P2_MIN_C2C
-#define PF_P2_MIN_C2C 3
+#define PF_P2_MIN_C2C 4
 #endif
 #ifndef PF_P2_MIN_C2R
 #define PF_P2_MIN_C2R 3
+#endif
+#ifndef PF_P2_MIN_MID
+#define PF_P2_MIN_MID 3
 #endif
 
 struct P2 {
@@ -787,7 +795,7 @@ __global__ void __launch_bounds__(kP2Threads, 2)
 // staying in shared memory between the two (tables of both directions in shared memory).
 // ---------------------------------------------------------------------------
 template <int L, class Mid>
-__global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
+__global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_MID)
     kp2_c2c_mid(const float4* __restrict__ twf, const float4* __restrict__ twb, long long ntiles, int tpo,
                 int Lout, P2ArrLoad ld, Mid mid, P2ArrStore st) {
   using G = P2Geom<L>;
