@@ -1162,7 +1162,7 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
     P->grid_cap = P->tune_grid[2];
     const size_t left = (size_t)(g.domain - (size_t)(dst - out));
     if constexpr (F32) {
-      if (P->tune_variant[2] == 0 && g.T[0] % 2 == 0 && p2_length(g.T[0] / 2)) {
+      if (P->tune_variant[2] != 1 && g.T[0] % 2 == 0 && p2_length(g.T[0] / 2)) {
         P2RowLoad rl;
         rl.ptr = (const float2*)src;
         rl.rowstride = (unsigned)P0;
@@ -1178,6 +1178,8 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
         ps.np = (int)nrows;
         ps.Lout = g.n[0];
         ps.vec = (g.n[0] % 2 == 0 && ((uintptr_t)dst & 7u) == 0) ? 1 : 0;
+        if (P->tune_variant[2] == 2 && p2_bulk_ok(rl, g.T[0] / 2))  // rows staged by bulk copies
+          return p2_c2r_bulk(P, "gen_c2r_d0_bulk", g.T[0] / 2, g.n[0], nrows, rl, ps, b3);
         return p2_c2r(P, "gen_c2r_d0", g.T[0] / 2, g.n[0], nrows, rl, ps, b3);
       }
     }

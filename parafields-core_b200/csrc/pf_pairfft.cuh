@@ -882,6 +882,118 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2R)
   p2_report(bad);
 }
 
+// ---------------------------------------------------------------------------
+// Complex-to-real rows with the rows staged by bulk copies.  A tile's NP rows are adjacent
+// in memory (row stride `rowstride` complex, 16-byte multiple), so one cp.async.bulk per
+// tile moves them into shared memory, completion counted on an mbarrier; two tile buffers
+// alternate over the persistent loop, so the next tile's copy runs while the current one
+// is transformed, and each input element is read from HBM once (the scalar kernel reads X[m]
+// and X[L-m] as separate loads).  Rows beyond the last row read as zero; a copy whose rows
+// would leave the buffer is not issued (bit 1 of the error word, zero rows).  Every wait is
+// bounded: a wait that gives up sets bit 2 and the CTA leaves the loop (all threads together).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"((uint64_t)__cvta_generic_to_global(src)), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+template <int L>
+struct P2Bulk {
+  // shared memory of kp2_c2r_bulk for rows of `rowstride` complex
+  static size_t smem_bytes(unsigned rowstride) {
+    using G = P2Geom<L>;
+    return 2 * (size_t)G::NP * rowstride * 8 + (size_t)(G::Q * G::PLQ + G::NTW + L) * 16 + 2 * 8;
+  }
+};
+
+template <int L, class St>
+__global__ void __launch_bounds__(kP2Threads, 2)
+    kp2_c2r_bulk(const float4* __restrict__ twg, long long ntiles, int Lout, P2RowLoad ld, St st) {
+  using G = P2Geom<L>;
+  extern __shared__ __align__(128) float4 p2_bulk_smem[];
+  const unsigned rs = ld.rowstride;
+  const unsigned tile_f2 = (unsigned)G::NP * rs;  // complex per tile buffer (rs even: 16-byte multiple)
+  float2* tb0 = reinterpret_cast<float2*>(p2_bulk_smem);
+  float2* tb1 = tb0 + tile_f2;
+  float4* buf = reinterpret_cast<float4*>(tb1 + tile_f2);
+  float4* tw = buf + G::Q * G::PLQ;
+  const float4* twT = tw + G::NTW;  // exp(+2 pi i m / 2L), m < L
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + G::NTW + L);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  p2_copy_table(tw, twg, G::NTW + L);
+  __syncthreads();
+  const int u = tid % G::TP, q = tid / G::TP;
+  unsigned bad = 0;
+  auto issue = [&](long long t, int slot) {
+    const long long p0 = t * G::NP;
+    const long long nrows = ld.np - p0 < G::NP ? ld.np - p0 : G::NP;
+    const unsigned long long top = (unsigned long long)(p0 + nrows) * rs;
+    const bool ok = nrows > 0 && top <= (unsigned long long)ld.n;
+    bad |= (unsigned)(nrows > 0 && !ok);
+    const uint32_t bytes = ok ? (uint32_t)(nrows * rs * 8) : 0u;
+    float2* dst = slot ? tb1 : tb0;
+    fence_proxy_async();  // the buffer's previous contents were read through the generic proxy
+    mbar_expect_tx(&bar[slot], bytes);
+    if (bytes) bulk_load(dst, ld.ptr + (unsigned long long)p0 * rs, bytes, &bar[slot]);
+  };
+  long long tile = blockIdx.x;
+  if (tid == 0 && tile < ntiles) issue(tile, 0);
+  int k = 0;
+  bool pending_next = false;
+  for (; tile < ntiles; tile += gridDim.x, k++) {
+    const int slot = k & 1;
+    const long long next = tile + gridDim.x;
+    pending_next = next < ntiles;
+    // the other buffer was last read before a barrier of the previous tile's transform
+    if (tid == 0 && pending_next) issue(next, slot ^ 1);
+    const bool ok = mbar_wait_bounded(&bar[slot], (uint32_t)(k >> 1) & 1u);
+    if (!__syncthreads_and(ok)) {
+      bad |= 2u;
+      break;
+    }
+    pending_next = false;
+    const long long p0 = tile * G::NP;
+    const int p = (int)p0 + 2 * q;
+    const float2* ra = (slot ? tb1 : tb0) + (unsigned)(2 * q) * rs;
+    const float2* rb = ra + rs;
+    const bool va = p < ld.np, vb = p + 1 < ld.np;
+    const float2 z2 = make_float2(0.f, 0.f);
+    P2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const int m = u + r * G::TP;
+      const bool im = m < ld.Lin, iy = L - m < ld.Lin;
+      float2 xa = va && im ? ra[m] : z2, xb = vb && im ? rb[m] : z2;
+      float2 ya = va && iy ? ra[L - m] : z2, yb = vb && iy ? rb[L - m] : z2;
+      if (m == 0) {
+        xa.y = 0.f;
+        xb.y = 0.f;
+        ya.y = 0.f;
+        yb.y = 0.f;
+      }
+      const P2 X = p2_ab(xa, xb), Y = p2_ab(ya, yb);
+      // s = X + conj(Y), d = X - conj(Y), t = d w, Z = s + i t
+      const P2 s = {f2add(X.re, Y.re), f2sub(X.im, Y.im)};
+      const P2 d = {f2sub(X.re, Y.re), f2add(X.im, Y.im)};
+      const P2 t = ptw(d, twT[m]);
+      v[r] = {f2sub(s.re, t.im), f2add(s.im, t.re)};
+    }
+    p2_transform<L, +1>(v, buf, tw, u, q, [&](int m, const P2& z) {
+      if (2 * m < Lout) st.store(p, m, z, bad);
+    });
+  }
+  if ((bad & 2u) && tid == 0 && pending_next)  // a copy issued before the failed wait: bounded wait for it
+    mbar_wait_bounded(&bar[(k & 1) ^ 1], (uint32_t)((k + 1) >> 1) & 1u);
+  p2_report(bad);
+}
+
 // field rows of n0 reals (row p at p * n0), value transform applied
 struct P2FieldStore {
   float* out;

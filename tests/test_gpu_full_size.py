@@ -335,6 +335,81 @@ def test_tma_staged_strided_pass(oracle, name):
     pfb200.wisdom_forget()
 
 
+BULK = {"2d-128": dict(dim=2, cells=(128, 40), covariance="exponential", corr_length=0.1),
+        "2d-128-ragged": dict(dim=2, cells=(128, 37), covariance="gaussian", corr_length=0.2, approximate=True)}
+
+
+@pytest.mark.parametrize("name", ["c2", "2d-128", "2d-128-ragged", "2d-exp-1024", "2d-m32-geo-2048",
+                                  "2d-exp-c2r-2048"])
+def test_bulk_staged_c2r_pass(oracle, name):
+    """The complex-to-real pass with its rows staged by bulk copies (tuning variant 2 of the
+    last pass) gives the oracle's realizations at every paired length (128..2048 points) and
+    with a last tile of fewer rows than a full one."""
+    cfgs = dict(LONG, c2=C2, **BULK)
+    d = desc_of(cfgs[name], precision=pfb200.PREC_F32)
+    g = oracle.resolve(d)
+    lam, _, _ = oracle.spectrum(d)
+    P = pfb200.Plan(d)
+    P.spectrum_build()
+    _force_variant(P, 2, 2)
+    P.profile(True)
+    P.generate(seed=1)
+    assert "gen_c2r_d0_bulk" in [r["name"] for r in P.profile_read()]  # the bulk-staged kernel ran
+    P.profile(False)
+    for seed in (5, 6):
+        ref, _ = oracle.generate(d, lam, counter_noise(g, seed, False))
+        assert rel(P.generate(seed=seed), ref) < TOL32, seed
+    noise = oracle.noise(3, g.noise)
+    ref, _ = oracle.generate(d, lam, noise)
+    assert rel(P.generate(noise=noise), ref) < TOL32
+    P.close()
+    pfb200.wisdom_forget()
+
+
+def _force_groups(P, groups, variants=None):
+    """measured planning, then the plane groups (pass 3 wisdom entry) and optionally the
+    variants of passes 1 and 2 replaced"""
+    pfb200.wisdom_forget()
+    P.autotune(repetitions=1)
+    out = []
+    for line in pfb200.wisdom_export().strip().splitlines():
+        f = line.split()
+        if f[0] == "3":
+            f[6] = str(groups)
+        if variants and int(f[0]) in variants:
+            f[5] = str(variants[int(f[0])])
+        out.append(" ".join(f))
+    pfb200.wisdom_forget()
+    pfb200.wisdom_import("\n".join(out) + "\n")
+    assert P.autotune() is False
+
+
+@pytest.mark.parametrize("case", [("c2", pfb200.PREC_F32, 3, None), ("c2", pfb200.PREC_F32, 8, {1: 2, 2: 2}),
+                                  ("3d-small", pfb200.PREC_F64, 5, None),
+                                  ("3d-small", pfb200.PREC_F32, 64, {1: 1, 2: 1})])
+def test_plane_groups(oracle, case):
+    """The last two 3D passes over groups of output planes (a group count that does not
+    divide the planes, more groups than planes, paired / staged / scalar kernels, FP32 and
+    FP64): bit-identical to one group, and equal to the oracle."""
+    name, prec, groups, variants = case
+    cfg = C2 if name == "c2" else dict(dim=3, cells=(40, 24, 36), covariance="matern32", corr_length=0.15,
+                                       approximate=True)
+    d = desc_of(cfg, precision=prec)
+    g = oracle.resolve(d)
+    lam, _, _ = oracle.spectrum(d)
+    P = pfb200.Plan(d)
+    P.spectrum_build()
+    _force_groups(P, 1, variants)
+    one = P.generate(seed=11)
+    _force_groups(P, groups, variants)
+    many = P.generate(seed=11)
+    assert np.array_equal(one, many)
+    ref, _ = oracle.generate(d, lam, counter_noise(g, 11, prec == pfb200.PREC_F64))
+    assert rel(many, ref) < (TOL32 if prec == pfb200.PREC_F32 else TOL64F)
+    P.close()
+    pfb200.wisdom_forget()
+
+
 @pytest.mark.parametrize("name,prec", [("c2", pfb200.PREC_F32), ("2d-exp-1024", pfb200.PREC_F32),
                                        ("2d-exp-1024", pfb200.PREC_F64), ("3d-exp-d1-1024", pfb200.PREC_F64)])
 def test_exported_noise_reproduces_seeded_realizations(oracle, name, prec):
