@@ -262,6 +262,11 @@ struct pf_plan {
   // output planes in turn, so that the intermediate between them (one group, held in a
   // buffer reused by every group) stays in L2 instead of crossing HBM twice; 1 = one group
   int gen_chunks = 1;
+  // tile counters of the dynamically ordered paired passes: [kind (0 noise, 1 strided)]
+  // [slot], the slot being the batch lane of the realization (0 outside batches), so that
+  // kernels that run at the same time never share a counter
+  unsigned long long* tile_ctr = nullptr;
+  int ctr_slot = 0;
 };
 
 static pf_status dalloc(pf_plan* P, void** p, size_t bytes) {
@@ -1524,6 +1529,7 @@ static pf_status generate_stage_pipeline(pf_plan* P, uint64_t seed, int32_t coun
         std::swap(P->ws[0], P->ws_b[0]);
         std::swap(P->ws_bytes[0], P->ws_b_bytes[0]);
       }
+      P->ctr_slot = slot;
       void* dst = (char*)out + (size_t)r * bytes;
       const pf_status s2 = f64 ? gen_r2c<double, double>(P, nullptr, seed + r, (double*)dst, tr, stages)
                                : gen_r2c<float, float>(P, nullptr, seed + r, (float*)dst, tr, stages);
@@ -1531,6 +1537,7 @@ static pf_status generate_stage_pipeline(pf_plan* P, uint64_t seed, int32_t coun
         std::swap(P->ws[0], P->ws_b[0]);
         std::swap(P->ws_bytes[0], P->ws_b_bytes[0]);
       }
+      P->ctr_slot = 0;
       return s2;
     };
     P->stream = P->lane[0];
@@ -1639,7 +1646,8 @@ void pf_plan_destroy(pf_plan* P) {
       for (int o = 0; o < 4; o++) P->fac[a][o] = nullptr;
   }
   void** bufs[] = {(void**)&P->lam64, (void**)&P->sq64, (void**)&P->sq32, (void**)&P->lam32, (void**)&P->scan,
-                   (void**)&P->cof, &P->ws[0], &P->ws[1], &P->ws[2], (void**)&P->noise_dev, &P->io_dev, &P->io2_dev, &P->spare};
+                   (void**)&P->cof, &P->ws[0], &P->ws[1], &P->ws[2], (void**)&P->noise_dev, &P->io_dev, &P->io2_dev, &P->spare,
+                   (void**)&P->tile_ctr};
   for (void** b : bufs)
     if (*b) cudaFree(*b), *b = nullptr;
   for (int a = 0; a < 2; a++)
@@ -1816,8 +1824,10 @@ pf_status pf_generate_batch(pf_plan* P, uint64_t seed, int32_t count, void* out,
           std::swap(P->ws_bytes[i], P->ws_b_bytes[i]);
         }
       P->stream = P->lane[slot];
+      P->ctr_slot = slot;
       st = es == 8 ? gen_r2c<double, double>(P, nullptr, seed + r, (double*)dst, tr)
                    : gen_r2c<float, float>(P, nullptr, seed + r, (float*)dst, tr);
+      P->ctr_slot = 0;
       if (st == PF_OK && host &&
           cudaMemcpyAsync((char*)out + (size_t)r * bytes, dst, bytes, cudaMemcpyDeviceToHost, P->lane[slot]) !=
               cudaSuccess)

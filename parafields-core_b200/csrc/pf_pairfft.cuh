@@ -607,9 +607,35 @@ struct P2Noise {
   }
 };
 
+// Tile order of the persistent passes.  With a counter (zeroed in the stream before the
+// launch) every CTA takes its next tile index from it, so CTAs on SMs that run faster take
+// more tiles and the launch ends when the work does (the noise pass alone: 0.263 against 0.284
+// ms with the static order on the 256^3 workload).  Thread 0 fetches the index of the next
+// tile while the current one is transformed; the other threads read it after the barrier at
+// the end of the tile (every tile body passes barriers after the previous read of *s).
+// Without a counter the CTAs stride over the tiles by the grid size.
+__device__ __forceinline__ long long tile_first(unsigned long long* ctr, long long* s) {
+  if (!ctr) return blockIdx.x;
+  if (threadIdx.x == 0) *s = (long long)atomicAdd(ctr, 1ull);
+  __syncthreads();
+  return *s;
+}
+__device__ __forceinline__ unsigned long long tile_prefetch(unsigned long long* ctr) {
+  return (ctr && threadIdx.x == 0) ? atomicAdd(ctr, 1ull) : 0ull;
+}
+__device__ __forceinline__ long long tile_next(unsigned long long* ctr, long long* s, long long tile,
+                                               unsigned long long nxt) {
+  if (!ctr) return tile + gridDim.x;
+  if (threadIdx.x == 0) *s = (long long)nxt;
+  __syncthreads();
+  return *s;
+}
+
 template <int L, class Ld>
 __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
-    kp2_noise(const float4* __restrict__ twg, long long ntiles, int tpo, int Lout, Ld ld, P2ArrStore st) {
+    kp2_noise(const float4* __restrict__ twg, long long ntiles, int tpo, int Lout, Ld ld, P2ArrStore st,
+              unsigned long long* ctr) {
+  __shared__ long long s_tile;
   using G = P2Geom<L>;
   extern __shared__ __align__(16) float4 p2_smem[];
   float4* buf = p2_smem;
@@ -618,7 +644,8 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
   __syncthreads();
   const int q = threadIdx.x % G::Q, u = threadIdx.x / G::Q;
   unsigned bad = 0;
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  for (long long tile = tile_first(ctr, &s_tile); tile < ntiles;) {
+    const unsigned long long nxt = tile_prefetch(ctr);
     const int o = (int)(tile / tpo);
     const int p = (int)(tile - (long long)o * tpo) * G::NP + 2 * q;
     P2 v[8];
@@ -634,6 +661,7 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
     p2_transform<L, +1>(v, buf, tw, u, q, [&](int j, const P2& x) {
       if (j < Lout) st.store_t(so, j, x);
     });
+    tile = tile_next(ctr, &s_tile, tile, nxt);
   }
   p2_report(bad);
 }
@@ -643,7 +671,9 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
 // ---------------------------------------------------------------------------
 template <int L, int S>
 __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
-    kp2_c2c(const float4* __restrict__ twg, long long ntiles, int tpo, int Lout, P2ArrLoad ld, P2ArrStore st) {
+    kp2_c2c(const float4* __restrict__ twg, long long ntiles, int tpo, int Lout, P2ArrLoad ld, P2ArrStore st,
+            unsigned long long* ctr) {
+  __shared__ long long s_tile;
   using G = P2Geom<L>;
   extern __shared__ __align__(16) float4 p2_smem[];
   float4* buf = p2_smem;
@@ -652,7 +682,8 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
   __syncthreads();
   const int q = threadIdx.x % G::Q, u = threadIdx.x / G::Q;
   unsigned bad = 0;
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  for (long long tile = tile_first(ctr, &s_tile); tile < ntiles;) {
+    const unsigned long long nxt = tile_prefetch(ctr);
     const int o = (int)(tile / tpo);
     const int p = (int)(tile - (long long)o * tpo) * G::NP + 2 * q;
     P2 v[8];
@@ -663,6 +694,7 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
     p2_transform<L, S>(v, buf, tw, u, q, [&](int j, const P2& x) {
       if (j < Lout) st.store_t(so, j, x);
     });
+    tile = tile_next(ctr, &s_tile, tile, nxt);
   }
   p2_report(bad);
 }
