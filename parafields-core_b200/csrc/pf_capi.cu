@@ -1356,11 +1356,44 @@ static pf_status matvec_r2c(pf_plan* P, int op, const S* in, S* out) {
   const double lb = sizeof(T);
   FieldRowLoad<S> fl{in, g.n[0], (unsigned)g.domain};
   FieldRowStore<S> fs{out, g.n[0], 0, 0.0, (unsigned)g.domain};
+  // the real-to-complex and complex-to-real rows along dim 0 take the paired kernels where
+  // T0/2 is a power of two in [128, 2048] (FP32 transforms)
+  const bool p2rows = std::is_same<T, float>::value && g.T[0] % 2 == 0 && p2_length(g.T[0] / 2);
+  const int pair_ok = (g.n[0] % 2 == 0) ? 1 : 0;
+  auto fwd_rows = [&](void* X, long long nrows) -> pf_status {
+    const double b = (double)nrows * (g.n[0] * sizeof(S) + T0c * e);
+    if constexpr (std::is_same<T, float>::value) {
+      if (p2rows) {
+        P2RealRowLoad<S> rl{in, g.n[0], (unsigned)g.domain, (int)nrows,
+                            pair_ok && ((uintptr_t)in % (2 * sizeof(S))) == 0 ? 1 : 0};
+        P2RowStore rs{(float2*)X, (unsigned)P0, (unsigned)std::min<size_t>(cap_of(P, X) / sizeof(float2), 0xffffffffu),
+                      (int)nrows, T0c};
+        return p2_r2c(P, "mv_r2c_d0", g.T[0] / 2, nrows, rl, rs, b);
+      }
+    }
+    return run_freal<T, true>(P, "mv_r2c_d0", g.T[0], T0c, nrows, fl, arr_store<cx<T>>(P, X, 1, 0, P0), b);
+  };
+  auto inv_rows = [&](void* X, long long nrows) -> pf_status {
+    const double b = (double)nrows * (T0c * e + g.n[0] * sizeof(S));
+    if constexpr (std::is_same<T, float>::value) {
+      if (p2rows) {
+        P2RowLoad rl;
+        rl.ptr = (const float2*)X;
+        rl.rowstride = (unsigned)P0;
+        rl.n = (unsigned)std::min<size_t>(cap_of(P, X) / sizeof(float2), 0xffffffffu);
+        rl.Lin = T0c;
+        rl.np = (int)nrows;
+        P2FieldStoreT<S> ps{out, g.n[0], 0, 0.f, (unsigned)g.domain, (int)nrows, g.n[0],
+                            pair_ok && ((uintptr_t)out % (2 * sizeof(S))) == 0 ? 1 : 0};
+        return p2_c2r(P, "mv_c2r_d0", g.T[0] / 2, g.n[0], nrows, rl, ps, b);
+      }
+    }
+    return run_freal<T, false>(P, "mv_c2r_d0", g.T[0], g.n[0], nrows, arr_load<cx<T>>(P, X, 1, 0, P0, T0c), fs, b);
+  };
   if (g.dim == 2) {
     void* X1 = nullptr;
     TRY(workspace(P, 2, sizeof(cx<T>) * (size_t)P0 * g.n[1], &X1));
-    TRY((run_freal<T, true>(P, "mv_r2c_d0", g.T[0], T0c, g.n[1], fl, arr_store<cx<T>>(P, X1, 1, 0, P0),
-                            (double)g.n[1] * (g.n[0] * sizeof(S) + T0c * e))));
+    TRY(fwd_rows(X1, g.n[1]));
     const double bf1 = (double)T0c * (2.0 * g.n[1] * e + g.T[1] * lb);
     if (std::is_same<T, float>::value && p2_length(g.T[1]) && p2_view_ok(X1, P0, 0, 1))
       TRY(p2_c2c_mid(P, "mv_fused_d1", g.T[1], g.n[1], T0c, 1, p2_load(P, X1, P0, 0, g.n[1], T0c), mid,
@@ -1369,20 +1402,27 @@ static pf_status matvec_r2c(pf_plan* P, int op, const S* in, S* out) {
       TRY((run_fpass<T, -1, +1, false, false>(P, "mv_fused_d1", g.T[1], g.n[1], T0c, 1,
                                               arr_load<cx<T>>(P, X1, P0, 0, 1, g.n[1]), mid,
                                               arr_store<cx<T>>(P, X1, P0, 0, 1), bf1)));
-    return run_freal<T, false>(P, "mv_c2r_d0", g.T[0], g.n[0], g.n[1], arr_load<cx<T>>(P, X1, 1, 0, P0, T0c), fs,
-                               (double)g.n[1] * (T0c * e + g.n[0] * sizeof(S)));
+    return inv_rows(X1, g.n[1]);
   }
   void *X1 = nullptr, *X2 = nullptr;
   TRY(workspace(P, 1, sizeof(cx<T>) * (size_t)P0 * g.n[1] * g.n[2], &X1));
   TRY(workspace(P, 2, sizeof(cx<T>) * (size_t)P0 * g.T[1] * g.n[2], &X2));
   const long long rows = (long long)g.n[1] * g.n[2];
   const long long s2 = (long long)P0 * g.T[1];
-  TRY((run_freal<T, true>(P, "mv_r2c_d0", g.T[0], T0c, rows, fl, arr_store<cx<T>>(P, X1, 1, 0, P0),
-                          (double)rows * (g.n[0] * sizeof(S) + T0c * e))));
-  TRY((run_fpass<T, -1, -1, false, false>(P, "mv_c2c_d1", g.T[1], g.T[1], T0c, g.n[2],
-                                          arr_load<cx<T>>(P, X1, P0, (long long)P0 * g.n[1], 1, g.n[1]), NoMid(),
-                                          arr_store<cx<T>>(P, X2, P0, s2, 1),
-                                          (double)T0c * g.n[2] * (g.n[1] + g.T[1]) * e)));
+  TRY(fwd_rows(X1, rows));
+  // the strided passes along dim 1 take the paired kernels where the torus length and the
+  // views allow (FP32 transforms), as in generation
+  const long long w1o = (long long)P0 * g.n[1];
+  const bool p2d1 = std::is_same<T, float>::value && p2_length(g.T[1]) && p2_view_ok(X1, P0, w1o, g.n[2]) &&
+                    p2_view_ok(X2, P0, s2, g.n[2]);
+  const double bd1 = (double)T0c * g.n[2] * (g.n[1] + g.T[1]) * e;
+  if (p2d1)
+    TRY(p2_c2c<-1>(P, "mv_c2c_d1", g.T[1], g.T[1], T0c, g.n[2], p2_load(P, X1, P0, w1o, g.n[1], T0c),
+                   p2_store(P, X2, P0, s2, T0c), bd1));
+  else
+    TRY((run_fpass<T, -1, -1, false, false>(P, "mv_c2c_d1", g.T[1], g.T[1], T0c, g.n[2],
+                                            arr_load<cx<T>>(P, X1, P0, w1o, 1, g.n[1]), NoMid(),
+                                            arr_store<cx<T>>(P, X2, P0, s2, 1), bd1)));
   // forward along dim 2, eigenvalue factor, backward along dim 2 (pencils k0 x k1)
   const double bf2 = (double)T0c * g.T[1] * (2.0 * g.n[2] * e + g.T[2] * lb);
   if (std::is_same<T, float>::value && p2_length(g.T[2]) && p2_view_ok(X2, s2, P0, g.T[1]))
@@ -1392,12 +1432,14 @@ static pf_status matvec_r2c(pf_plan* P, int op, const S* in, S* out) {
     TRY((run_fpass<T, -1, +1, false, false>(P, "mv_fused_d2", g.T[2], g.n[2], T0c, g.T[1],
                                             arr_load<cx<T>>(P, X2, s2, P0, 1, g.n[2]), mid,
                                             arr_store<cx<T>>(P, X2, s2, P0, 1), bf2)));
-  TRY((run_fpass<T, +1, +1, false, false>(P, "mv_c2c_d1i", g.T[1], g.n[1], T0c, g.n[2],
-                                          arr_load<cx<T>>(P, X2, P0, s2, 1, g.T[1]), NoMid(),
-                                          arr_store<cx<T>>(P, X1, P0, (long long)P0 * g.n[1], 1),
-                                          (double)T0c * g.n[2] * (g.n[1] + g.T[1]) * e)));
-  return run_freal<T, false>(P, "mv_c2r_d0", g.T[0], g.n[0], rows, arr_load<cx<T>>(P, X1, 1, 0, P0, T0c), fs,
-                             (double)rows * (T0c * e + g.n[0] * sizeof(S)));
+  if (p2d1)
+    TRY(p2_c2c<+1>(P, "mv_c2c_d1i", g.T[1], g.n[1], T0c, g.n[2], p2_load(P, X2, P0, s2, g.T[1], T0c),
+                   p2_store(P, X1, P0, w1o, T0c), bd1));
+  else
+    TRY((run_fpass<T, +1, +1, false, false>(P, "mv_c2c_d1i", g.T[1], g.n[1], T0c, g.n[2],
+                                            arr_load<cx<T>>(P, X2, P0, s2, 1, g.T[1]), NoMid(),
+                                            arr_store<cx<T>>(P, X1, P0, w1o, 1), bd1)));
+  return inv_rows(X1, rows);
 }
 
 // DFT field backend matvec: complex embedding, c2c on every axis, Re extraction

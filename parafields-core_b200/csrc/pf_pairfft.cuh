@@ -829,7 +829,8 @@ __global__ void __launch_bounds__(kP2Threads, 2)
 template <int L, class Mid>
 __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_MID)
     kp2_c2c_mid(const float4* __restrict__ twf, const float4* __restrict__ twb, long long ntiles, int tpo,
-                int Lout, P2ArrLoad ld, Mid mid, P2ArrStore st) {
+                int Lout, P2ArrLoad ld, Mid mid, P2ArrStore st, unsigned long long* ctr) {
+  __shared__ long long s_tile;
   using G = P2Geom<L>;
   extern __shared__ __align__(16) float4 p2_smem[];
   float4* buf = p2_smem;
@@ -840,7 +841,8 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_MID)
   __syncthreads();
   const int q = threadIdx.x % G::Q, u = threadIdx.x / G::Q;
   unsigned bad = 0;
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  for (long long tile = tile_first(ctr, &s_tile); tile < ntiles;) {
+    const unsigned long long nxt = tile_prefetch(ctr);
     const int o = (int)(tile / tpo);
     const int p = (int)(tile - (long long)o * tpo) * G::NP + 2 * q;
     P2 v[8];
@@ -865,6 +867,7 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_MID)
     p2_transform<L, +1>(v, buf, tb, u, q, [&](int j, const P2& x) {
       if (j < Lout) st.store_t(so, j, x);
     });
+    tile = tile_next(ctr, &s_tile, tile, nxt);
   }
   p2_report(bad);
 }
@@ -1026,16 +1029,19 @@ __global__ void __launch_bounds__(kP2Threads, 2)
   p2_report(bad);
 }
 
-// field rows of n0 reals (row p at p * n0), value transform applied
-struct P2FieldStore {
-  float* out;
+// field rows of n0 reals (row p at p * n0) of type O (FP32 fields, or the FP64 vectors of
+// the matvec and the CG), value transform applied in FP32
+template <typename O>
+struct P2FieldStoreT {
+  using O2 = typename std::conditional<sizeof(O) == 8, double2, float2>::type;
+  O* out;
   int n0;
   int transform;
   float boxcox;
   unsigned n;
   int np;
   int Lout;
-  int vec;  // out is 8-byte aligned and n0 is even: pairs are stored as float2
+  int vec;  // out is aligned for pairs (8 bytes FP32, 16 bytes FP64) and n0 is even
   __device__ __forceinline__ void row(int p, int m, float a, float b, unsigned& bad) const {
     if (p >= np) return;
     if (transform) {
@@ -1047,11 +1053,14 @@ struct P2FieldStore {
     const bool ok = i + (two ? 1u : 0u) < n;
     bad |= (unsigned)!ok;
     if (!ok) return;
-    if (two && vec)
-      *reinterpret_cast<float2*>(out + i) = make_float2(a, b);
-    else {
-      out[i] = a;
-      if (two) out[i + 1] = b;
+    if (two && vec) {
+      O2 v;
+      v.x = (O)a;
+      v.y = (O)b;
+      *reinterpret_cast<O2*>(out + i) = v;
+    } else {
+      out[i] = (O)a;
+      if (two) out[i + 1] = (O)b;
     }
   }
   __device__ __forceinline__ void store(int p, int m, const P2& z, unsigned& bad) const {
@@ -1059,5 +1068,109 @@ struct P2FieldStore {
     row(p + 1, m, z.re.y, z.im.y, bad);
   }
 };
+using P2FieldStore = P2FieldStoreT<float>;
+
+// ---------------------------------------------------------------------------
+// Real-to-complex rows (L+1 complex from 2L reals, FFTW r2c semantics), the forward
+// transform of the matvec (r2cfieldbackend.hh:210-239 after fieldToExtendedField): rows p and
+// p+1 per pair, threads along the row.  The 2L reals x of a row (the n0 field values, zero
+// beyond) are transformed as the L complex z[m] = x[2m] + i x[2m+1]; with Z the forward
+// length-L transform of z (in shared memory after the last stage),
+//   X[k] = E - i w^k O,  E = (Z[k] + conj Z[L-k]) / 2,  O = (Z[k] - conj Z[L-k]) / 2,
+// w = exp(-2 pi i / 2L), for k = 0..L (Z[L] = Z[0]).
+// ---------------------------------------------------------------------------
+// rows p and p+1 of n0 reals of type S (row p at p * n0)
+template <typename S>
+struct P2RealRowLoad {
+  using S2 = typename std::conditional<sizeof(S) == 8, double2, float2>::type;
+  const S* x;
+  int n0;
+  unsigned n;
+  int np;
+  int vec;  // x is aligned for pairs (8 bytes FP32, 16 bytes FP64) and n0 is even
+  // (x[2m], x[2m+1]) of row p, zero beyond the row and beyond the last row
+  __device__ __forceinline__ float2 pair(int p, int m, unsigned& bad) const {
+    float2 z = make_float2(0.f, 0.f);
+    if (p >= np || 2 * m >= n0) return z;
+    const unsigned i = (unsigned)p * (unsigned)n0 + 2u * (unsigned)m;
+    const bool two = 2 * m + 1 < n0;
+    const bool ok = i + (two ? 1u : 0u) < n;
+    bad |= (unsigned)!ok;
+    if (!ok) return z;
+    if (two && vec) {
+      const S2 v = *reinterpret_cast<const S2*>(x + i);
+      return make_float2((float)v.x, (float)v.y);
+    }
+    z.x = (float)x[i];
+    if (two) z.y = (float)x[i + 1];
+    return z;
+  }
+};
+
+// complex rows p, p+1 (element k of row p at p * rowstride + k), elements k < Lout
+struct P2RowStore {
+  float2* ptr;
+  unsigned rowstride;
+  unsigned n;
+  int np;
+  int Lout;
+  __device__ __forceinline__ void one(int p, int k, float2 v, unsigned& bad) const {
+    if (p >= np || k >= Lout) return;
+    const unsigned i = (unsigned)p * rowstride + (unsigned)k;
+    const bool ok = i < n;
+    bad |= (unsigned)!ok;
+    if (ok) ptr[i] = v;
+  }
+};
+
+template <int L, class Ld>
+__global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2R)
+    kp2_r2c(const float4* __restrict__ twg, long long ntiles, Ld ld, P2RowStore st) {
+  using G = P2Geom<L>;
+  extern __shared__ __align__(16) float4 p2_smem[];
+  float4* buf = p2_smem;
+  float4* tw = p2_smem + G::Q * G::PLQ;
+  const float4* twT = tw + G::NTW;  // exp(+2 pi i m / 2L), m < L
+  p2_copy_table(tw, twg, G::NTW + L);
+  __syncthreads();
+  const int u = threadIdx.x % G::TP, q = threadIdx.x / G::TP;
+  unsigned bad = 0;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int p = (int)tile * G::NP + 2 * q;
+    P2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const int m = u + r * G::TP;
+      v[r] = p2_ab(ld.pair(p, m, bad), ld.pair(p + 1, m, bad));
+    }
+    // forward transform; Z lands in the exchange buffer (its last stage has read the buffer
+    // and passed a barrier before the first output is written)
+    p2_transform<L, -1>(v, buf, tw, u, q, [&](int j, const P2& x) { buf[p2_slot(G::PLQ, q, j)] = slot_of(x); });
+    __syncthreads();
+    const float2 half = make_float2(0.5f, 0.5f);
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const int k = u + r * G::TP;
+      const P2 A = p2_of(buf[p2_slot(G::PLQ, q, k)]);
+      const P2 B = p2_of(buf[p2_slot(G::PLQ, q, (L - k) & (L - 1))]);
+      // E = (A + conj B) / 2, O = (A - conj B) / 2
+      const P2 E = {f2mul(half, f2add(A.re, B.re)), f2mul(half, f2sub(A.im, B.im))};
+      const P2 O = {f2mul(half, f2sub(A.re, B.re)), f2mul(half, f2add(A.im, B.im))};
+      // twT[k] = (c, s) = exp(+2 pi i k / 2L); X = (Er + c Oi - s Or, Ei - c Or - s Oi)
+      const float4 w = twT[k];
+      const float2 c = make_float2(w.x, w.y), sn = make_float2(w.z, w.w);
+      const float2 xr = f2add(E.re, f2sub(f2mul(c, O.im), f2mul(sn, O.re)));
+      const float2 xi = f2sub(E.im, f2fma(c, O.re, f2mul(sn, O.im)));
+      st.one(p, k, make_float2(xr.x, xi.x), bad);
+      st.one(p + 1, k, make_float2(xr.y, xi.y), bad);
+      if (k == 0) {  // Nyquist X[L] = Re Z[0] - Im Z[0] (real)
+        st.one(p, L, make_float2(A.re.x - A.im.x, 0.f), bad);
+        st.one(p + 1, L, make_float2(A.re.y - A.im.y, 0.f), bad);
+      }
+    }
+    __syncthreads();  // the buffer is read before the next tile's transform writes it
+  }
+  p2_report(bad);
+}
 
 }  // namespace pf

@@ -450,3 +450,54 @@ def test_exported_noise_states_ensemble_field_errors(oracle):
         assert rel(E.field(out, i), ref) < TOL32, i
         P.close()
     E.close()
+
+
+# matvec rows along dim 0 on the paired kernels (T0/2 = 128 .. 2048), the strided dim-1 pass
+# paired where T1 is a power of two >= 128
+ROWS = {
+    "2d-rows-128": dict(dim=2, cells=(128, 48), covariance="exponential", corr_length=0.1),
+    "2d-rows-512": dict(dim=2, cells=(512, 20), covariance="gaussian", corr_length=0.05, approximate=True),
+    "2d-rows-2048": dict(dim=2, cells=(2048, 8), covariance="exponential", corr_length=(0.05, 0.2),
+                         anisotropy="axiparallel"),
+    "3d-rows-d1": dict(dim=3, cells=(128, 64, 24), covariance="exponential",
+                       corr_length=(0.15, 0.02, 0.01, 0.02, 0.08, 0.0, 0.01, 0.0, 0.04), anisotropy="geometric",
+                       approximate=True),
+}
+
+
+@pytest.mark.parametrize("op", [pfb200.OP_MUL, pfb200.OP_ROOT, pfb200.OP_INVEXT])
+@pytest.mark.parametrize("name", list(ROWS))
+def test_fp32_matvec_paired_rows(oracle, name, op):
+    """FP32 matvec whose real-to-complex and complex-to-real rows run on the paired kernels
+    (kp2_r2c / kp2_c2r with the vector's type), against the FP64 oracle."""
+    d = desc_of(ROWS[name], precision=pfb200.PREC_F32)
+    lam, _, status = oracle.spectrum(d)
+    assert status == 0
+    if op == pfb200.OP_INVEXT and (lam <= 1e-6 * lam.max()).any():
+        pytest.skip("ill-conditioned torus inverse: FP32 transforms cannot reach the tolerance")
+    g = oracle.resolve(d)
+    P = pfb200.Plan(d)
+    P.spectrum_build()
+    x = np.random.default_rng(5).standard_normal(g.domain)
+    ref = oracle.matvec(d, lam, op, x)
+    P.profile(True)
+    out = P.matvec(x.astype(np.float32), op=op, precision=pfb200.PREC_F32)
+    assert {"mv_r2c_d0", "mv_c2r_d0"} <= {r["name"] for r in P.profile_read()}
+    assert rel(out, ref) < TOL32
+    P.close()
+
+
+@pytest.mark.parametrize("name", ["2d-rows-128", "3d-rows-d1"])
+def test_cg_fp32_inner_paired_rows(oracle, name):
+    """Residual-mode CG with FP32 inner matvecs on the paired row kernels (FP64 vectors in
+    and out): the oracle's FP64 matvec confirms the 1e-8 residual."""
+    d = desc_of(ROWS[name])
+    lam, _, _ = oracle.spectrum(d)
+    g = oracle.resolve(d)
+    P = pfb200.Plan(d)
+    P.spectrum_build()
+    b = np.random.default_rng(13).standard_normal(g.domain)
+    x, rep = P.multiply_inverse(b, mode=pfb200.CG_RESIDUAL, tolerance=1e-8, inner_fp32=True, max_iterations=20000)
+    assert rep["relative_residual"] <= 1e-8
+    assert rel(oracle.matvec(d, lam, pfb200.OP_MUL, x), b) <= 1.1e-8
+    P.close()
