@@ -18,7 +18,10 @@ struct CgScratch {
 };
 
 constexpr int kCgThreads = 256;
-constexpr int kCgBlocks = 296;  // 2 x 148 SMs: fixed, so the reduction order is fixed
+// 8 x 148 SMs (64 warps per SM, one load in flight per thread: enough to stream the FP64
+// vectors; 2 per SM ran the dot products at about a third of HBM bandwidth); fixed, so the
+// reduction order is fixed
+constexpr int kCgBlocks = 1184;
 
 // scalar slots
 enum CgSlot {
