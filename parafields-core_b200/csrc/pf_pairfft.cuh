@@ -29,7 +29,8 @@ constexpr int kP2Threads = 256;
 // and in the two-stream batch its CTAs fit beside the other stream's kernels (256^3
 // Matern-3/2 batch: 0.388 against 0.401 ms per realization).  At 64 registers the
 // complex-to-real pass spills and runs slower alone (0.088 against 0.077 ms) and in the
-// batch; the fused matvec pass spills too.  Both keep 3.
+// batch, so it keeps 3.  The fused matvec pass spills a few words at 64 registers but waits
+// on its gathers, and the extra warps win (128^3 C^-1: 0.066 against 0.075 ms).
 #ifndef PF_P2_MIN_NOISE
 #define PF_P2_MIN_NOISE 4
 #endif
@@ -40,7 +41,7 @@ constexpr int kP2Threads = 256;
 #define PF_P2_MIN_C2R 3
 #endif
 #ifndef PF_P2_MIN_MID
-#define PF_P2_MIN_MID 3
+#define PF_P2_MIN_MID 4
 #endif
 
 struct P2 {
