@@ -9,6 +9,12 @@ G=<plane groups>.  Passes not named take variant 0 at full occupancy.
 
   python parafields-core_b200/pass_profile.py --cells 256 256 256 --covariance matern32 \\
       --corr-length 0.2 0.1 0.05 --approximate --run 2=0 --run 2=2 --realizations 2
+
+With --matvec K the plan instead runs K FP32 matvecs on FP32 device vectors (the CG's inner
+products run the same kernels with FP64 vectors in and out), e.g. the 128^3 covariance-inverse workload with a geometric anisotropy:
+
+  python parafields-core_b200/pass_profile.py --cells 128 128 128 --covariance exponential \\
+      --corr-length <9 values of the matrix> --approximate --matvec 2
 """
 import argparse
 import os
@@ -60,12 +66,26 @@ def main(argv=None):
     ap.add_argument("--fp64", action="store_true")
     ap.add_argument("--run", action="append", default=[], help="PASS=VARIANT[:CTAS],...[,G=groups]")
     ap.add_argument("--realizations", type=int, default=2)
+    ap.add_argument("--matvec", type=int, default=0,
+                    help="instead of realizations: this many FP32 matvecs (C x) on FP32 device vectors")
     a = ap.parse_args(argv)
     import torch
 
     dim = len(a.cells)
     d = pfb200.make_desc(dim=dim, cells=a.cells, covariance=a.covariance, corr_length=a.corr_length,
                          approximate=a.approximate, precision=pfb200.PREC_F64 if a.fp64 else pfb200.PREC_F32)
+    if a.matvec:
+        P = pfb200.Plan(d)
+        P.spectrum_build()
+        n = P.info.domain_size
+        x = torch.randn(n, dtype=torch.float32, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(a.matvec):
+            P.matvec(x, op=pfb200.OP_MUL, precision=pfb200.PREC_F32, out=y)
+        torch.cuda.synchronize()
+        print("%d matvecs" % a.matvec, flush=True)
+        P.close()
+        return
     for run in a.run or ["0=0"]:
         choices, groups = parse_run(run)
         P = pfb200.Plan(d)
