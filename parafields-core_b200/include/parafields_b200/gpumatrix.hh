@@ -74,9 +74,13 @@ class GpuMatrix {
   mutable pf_plan_info info{};
   mutable bool valid = false;       // matrixBackend.valid(): spectrum built for this level
   mutable bool sparePending = false;  // DFT field backend: second field cached (matrix.hh:411-420)
+  PlanningKeys planning;             // fftw.measure / fftw.useWisdom
 
   void release() {
-    if (plan) pf_plan_destroy(plan);
+    if (plan) {
+      planning.exportWisdom();
+      pf_plan_destroy(plan);
+    }
     plan = nullptr;
   }
 
@@ -113,6 +117,8 @@ class GpuMatrix {
     covariance = (*traits).covariance;
     variance = (*traits).variance;
     const pf_field_desc d = descriptor();
+    planning = PlanningKeys::fromConfig((*traits).config);
+    planning.importWisdom();
     check(pf_plan_create(&d, &plan));
     check(pf_plan_get_info(plan, &info));
     valid = false;
@@ -173,6 +179,7 @@ class GpuMatrix {
       const std::vector<double> v = customCovarianceValues<dim, RF>(info, ext, (double)variance, corr, cov);
       check(pf_spectrum_build_values(plan, v.data(), v.size(), PF_MEM_HOST, &stats));
     }
+    planning.plan(plan);
     valid = true;
     sparePending = false;
   }

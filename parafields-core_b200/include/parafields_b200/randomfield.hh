@@ -22,6 +22,7 @@
 #include <fstream>
 #include <memory>
 #include <random>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -44,6 +45,46 @@ inline void check(pf_status st) {
   if (st == PF_ERR_NEG_EIGEN) throw NegativeEigenvalueError{msg};
   throw std::runtime_error{msg};
 }
+
+// fftw.measure / fftw.useWisdom (r2cfieldbackend.hh:75-96, 212-216): with fftw.measure the
+// realization passes of a plan are planned by measurement (pf_plan_autotune) once its
+// spectrum exists; with fftw.useWisdom the planning choices are read from this file when a
+// plan is made and written back when it is destroyed.  The file holds the library's own
+// wisdom text (pf_wisdom_export), so it is not the reference's FFTW wisdom file.
+inline const char* wisdomFileName() { return "wisdom-R2CField-b200.txt"; }
+
+struct PlanningKeys {
+  bool measure = false;
+  bool useWisdom = false;
+  template <typename Config>
+  static PlanningKeys fromConfig(const Config& config) {
+    PlanningKeys k;
+    k.measure = config.template get<bool>("fftw.measure", false);
+    k.useWisdom = config.template get<bool>("fftw.useWisdom", false);
+    return k;
+  }
+  void importWisdom() const {
+    if (!useWisdom) return;
+    std::ifstream f(wisdomFileName());
+    if (!f) return;  // no file yet: FFTW's import_wisdom_from_filename ignores it too
+    std::stringstream ss;
+    ss << f.rdbuf();
+    check(pf_wisdom_import(ss.str().c_str()));
+  }
+  void exportWisdom() const noexcept {
+    if (!useWisdom) return;
+    uint64_t need = 0;
+    if (pf_wisdom_export(nullptr, 0, &need) != PF_OK || need == 0) return;
+    std::string buf(need, '\0');
+    if (pf_wisdom_export(&buf[0], need, &need) != PF_OK) return;
+    std::ofstream f(wisdomFileName(), std::ofstream::trunc);
+    f << buf.c_str();
+  }
+  // after the spectrum was built
+  void plan(pf_plan* p) const {
+    if (measure) check(pf_plan_autotune(p, 0, nullptr));
+  }
+};
 
 // Configuration keys of the path -> descriptor (fieldtraits.hh:175-186, 229;
 // matrix.hh:232-260, 268-269, 479-493, 515-602; covariance.hh:33-128, 395-396, 515-516,
@@ -228,15 +269,31 @@ class GpuPlan {
   pf_field_desc desc_{};
   bool spare_pending_ = false;
   bool custom_ = false;
+  PlanningKeys planning_{};
+  bool planned_ = false;  // fftw.measure: the passes were planned for this matrix
+  bool hasValues_ = false;  // custom covariance: the spectrum was built from values
+
+  // fftw.measure once the matrix can be built (the built-in covariances build it lazily on
+  // first use; a custom covariance needs fillTransformedMatrix with its functor first)
+  void plan() {
+    if (planned_ || !planning_.measure || (custom_ && !hasValues_)) return;
+    planning_.plan(plan_);
+    planned_ = true;
+  }
 
  public:
-  GpuPlan(const pf_field_desc& d, bool customCovariance = false) : desc_(d), custom_(customCovariance) {
+  GpuPlan(const pf_field_desc& d, bool customCovariance = false, PlanningKeys planning = PlanningKeys{})
+      : desc_(d), custom_(customCovariance), planning_(planning) {
     if ((d.precision == PF_PREC_F64) != (sizeof(RF) == 8))
       throw std::runtime_error{"gpu.precision must match the field's value type"};
+    planning_.importWisdom();
     check(pf_plan_create(&d, &plan_));
     check(pf_plan_get_info(plan_, &info_));
   }
-  ~GpuPlan() { pf_plan_destroy(plan_); }
+  ~GpuPlan() {
+    planning_.exportWisdom();
+    pf_plan_destroy(plan_);
+  }
   GpuPlan(const GpuPlan&) = delete;
   GpuPlan& operator=(const GpuPlan&) = delete;
 
@@ -248,6 +305,8 @@ class GpuPlan {
     if (custom_) throw std::runtime_error{"you need to call fillMatrix with your covariance class as parameter"};
     pf_eig_stats s{};
     check(pf_spectrum_build(plan_, &s));
+    planned_ = false;
+    plan();
     spare_pending_ = false;
     return s;
   }
@@ -260,6 +319,9 @@ class GpuPlan {
                                                                   desc_.corr_length[0], covariance);
     pf_eig_stats s{};
     check(pf_spectrum_build_values(plan_, v.data(), v.size(), PF_MEM_HOST, &s));
+    hasValues_ = true;
+    planned_ = false;
+    plan();
     spare_pending_ = false;
     return s;
   }
@@ -269,6 +331,7 @@ class GpuPlan {
   // returned by the next call without drawing noise (matrix.hh:411-420)
   template <typename RNG>
   void generateField(RNG& rng, std::vector<RF>& data) {
+    plan();
     data.resize(info_.domain_size);
     std::vector<double> noise;
     if (!spare_pending_) {
@@ -380,7 +443,7 @@ class RandomField {
       cells_[i] = cells_[i] * mul / div;
       desc_.cells[i] = (int32_t)cells_[i];
     }
-    matrix_ = std::make_shared<GpuPlan<RF>>(desc_, custom_);
+    matrix_ = std::make_shared<GpuPlan<RF>>(desc_, custom_, PlanningKeys::fromConfig(config_));
   }
 
   // RandomField::refine / coarsen (randomfield.hh:880-1018), using the cached matrix-vector
@@ -454,7 +517,7 @@ class RandomField {
     transform_ = ValueTransform<RF>(desc_.transform, (RF)desc_.boxcox_lambda);
     const std::string cov = config.get<std::string>("stochastic.covariance");
     custom_ = cov == "custom-iso" || cov == "custom-aniso";
-    matrix_ = std::make_shared<GpuPlan<RF>>(desc_, custom_);
+    matrix_ = std::make_shared<GpuPlan<RF>>(desc_, custom_, PlanningKeys::fromConfig(config));
     cells_ = config.get<std::array<unsigned, dim>>("grid.cells");
     dataCells_ = cells_;
     ext_ = config.get<std::array<double, dim>>("grid.extensions");

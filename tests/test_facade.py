@@ -155,3 +155,26 @@ def test_facade_write_and_read_field_files(facade_exe, tmp_path):
     assert np.array_equal(a, b)
     field = pfb200.read_field(tmp_path / "saved", (24, 20, 12))
     assert field.size == 24 * 20 * 12 and np.isfinite(field).all()
+
+
+@pytest.mark.gpu
+def test_facade_fftw_measure_and_wisdom(facade_exe, tmp_path, oracle):
+    """fftw.measure plans the realization passes by measurement once the matrix exists;
+    fftw.useWisdom writes the planning choices to wisdom-R2CField-b200.txt in the working
+    directory when the matrix goes away and reads them back for the next one
+    (r2cfieldbackend.hh:75-96, 212-216).  The field is the oracle's either way."""
+    keys = ("grid.cells = 48 40\ngrid.extensions = 1 1\nstochastic.corrLength = 0.1\nstochastic.variance = 1\n"
+            "stochastic.covariance = exponential\nrandomField.cgIterations = 60\n"
+            "fftw.measure = true\nfftw.useWisdom = true\n")
+    ini = write_ini(tmp_path, keys)
+    d = desc_of(dict(dim=2, cells=(48, 40), covariance="exponential", corr_length=0.1))
+    lam, _, _ = oracle.spectrum(d)
+    for attempt in range(2):  # second run: the wisdom file exists and is read
+        r = subprocess.run([facade_exe, "run", ini, "17", str(tmp_path)], capture_output=True, text=True,
+                           cwd=str(tmp_path))
+        assert r.returncode == 0, r.stdout + r.stderr
+        wis = (tmp_path / "wisdom-R2CField-b200.txt").read_text().split("\n")
+        assert any(line.startswith("0 ") for line in wis) and any(line.startswith("2 ") for line in wis)
+        noise = np.fromfile(str(tmp_path / "noise.bin"), dtype=np.float64)
+        field, _ = oracle.generate(d, lam, noise)
+        assert rel(np.fromfile(str(tmp_path / "field.bin"), dtype=np.float64), field) < 1e-11
