@@ -474,7 +474,8 @@ static size_t smem_of(const PassArgs& a, bool contig, int elem) {
 
 template <typename K>
 static pf_status set_smem(K kernel, size_t smem) {
-  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // the 48 KB a CTA gets without the attribute include the kernel's static shared memory
+  if (smem > 40 * 1024) CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   return PF_OK;
 }
 
@@ -1151,7 +1152,7 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
   } cap_reset{P};
   P->grid_cap = P->tune_grid[0];
   if (!(stages & 1)) {
-  } else if (F32 && P->tune_variant[0] == 0 && p2_length(Tl) && p2_view_ok(W1, jst, P0, outer))
+  } else if (F32 && P->tune_variant[0] == 0 && (p2_length(Tl) || p2_length3(Tl)) && p2_view_ok(W1, jst, P0, outer))
     TRY(p2_noise(P, "gen_noise_last", Tl, g.n[last], T0c, outer, nz, p2_store(P, W1, jst, P0, T0c), b1));
   else if (Tl % 2 == 0)
     TRY((run_fpass<T, +1, +1, false, true>(P, "gen_noise_last", Tl, g.n[last], T0c, outer, nz, NoMid(),

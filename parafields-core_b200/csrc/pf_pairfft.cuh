@@ -668,6 +668,107 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
 }
 
 // ---------------------------------------------------------------------------
+// Generation pass 1 for last-axis lengths L = 3 M (M a power of two, 64..512): the
+// length-L backward transform split as
+//   X[3 k1 + k2] = sum_n1 W_M^(n1 k1) [ W_L^(n1 k2) sum_n2 x[n1 + M n2] W_3^(n2 k2) ],
+// i.e. a radix-3 step with twiddles, then three paired M-point transforms per pencil
+// pair (one per k2).  A tile holds PP pencil pairs: their noise is first generated into
+// shared memory (the exchange buffer, PP L slots), then every thread reads the three inputs
+// of its radix-3 butterflies, and thread slot q transforms sub-pencil k2 = q % 3 of pair
+// q / 3.  The block has exactly 3 PP M/8 threads.
+// ---------------------------------------------------------------------------
+template <int M>
+struct P2Geom3 {
+  using G = P2Geom<M>;
+  static constexpr int L = 3 * M;
+  static constexpr int PP = kP2Threads / (3 * G::TP);  // pencil pairs per tile
+  static constexpr int NT = PP * 3 * G::TP;            // threads per CTA
+  static constexpr int QS = 3 * PP;                    // sub-pencil slots
+  static_assert(PP >= 1 && QS <= G::Q, "sub-pencil slots fit the exchange buffer");
+  static_assert(PP * L <= G::Q * G::PLQ, "the tile's noise fits the exchange buffer");
+};
+
+template <int M, class Ld>
+__global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
+    kp2_noise3(const float4* __restrict__ twg, long long ntiles, int tpo, int Lout, Ld ld, P2ArrStore st,
+               unsigned long long* ctr) {
+  __shared__ long long s_tile;
+  using G = P2Geom<M>;
+  using G3 = P2Geom3<M>;
+  constexpr int L = G3::L;
+  extern __shared__ __align__(16) float4 p2_smem[];
+  float4* buf = p2_smem;  // exchange buffer; also the tile's noise, pair g at buf[g L + n]
+  float4* tw = p2_smem + G::Q * G::PLQ;
+  const float4* tw3 = tw + G::NTW;  // exp(+2 pi i n1 k2 / L) at (k2 - 1) M + n1, k2 = 1, 2
+  p2_copy_table(tw, twg, G::NTW + 2 * M);
+  __syncthreads();
+  const int tid = threadIdx.x;
+  const int q = tid % G3::QS, u = tid / G3::QS;  // transform: sub-pencil slot, column
+  const int pq = q / 3, k2 = q - 3 * (q / 3);
+  const int gp = tid / (3 * G::TP), gi = tid - gp * (3 * G::TP);  // generation: pair, index
+  const float2 hf = make_float2(-0.5f, -0.5f);
+  const float sq3 = k2 == 1 ? 0.86602540378443865f : -0.86602540378443865f;
+  const float2 s3 = make_float2(sq3, sq3);
+  unsigned bad = 0;
+  for (long long tile = tile_first(ctr, &s_tile); tile < ntiles;) {
+    const unsigned long long nxt = tile_prefetch(ctr);
+    const int o = (int)(tile / tpo);
+    const int p0 = (int)(tile - (long long)o * tpo) * (2 * G3::PP);
+    {  // noise x[n] of pair gp, elements j and j + L/2 per call
+      const int p = p0 + 2 * gp;
+      float4* xs = buf + gp * L;
+      if (ld.noise) {
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          const int j = gi + r * (3 * G::TP);
+          P2 x0, x1;
+          ld.template load2<L>(p, j, o, x0, x1, bad);
+          xs[j] = slot_of(x0);
+          xs[j + L / 2] = slot_of(x1);
+        }
+      } else {
+        const auto t = ld.template tile<L>(p, o, bad);
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          const int j = gi + r * (3 * G::TP);
+          P2 x0, x1;
+          ld.template load2t<L>(t, j, x0, x1);
+          xs[j] = slot_of(x0);
+          xs[j + L / 2] = slot_of(x1);
+        }
+      }
+    }
+    __syncthreads();
+    // radix-3 step of sub-pencil k2 and its twiddle W_L^(n1 k2)
+    P2 v[8];
+    const float4* xs = buf + pq * L;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const int n1 = u + r * G::TP;
+      const P2 a = p2_of(xs[n1]), b = p2_of(xs[n1 + M]), c = p2_of(xs[n1 + 2 * M]);
+      const P2 sm = padd(b, c);
+      if (k2 == 0) {
+        v[r] = padd(a, sm);
+      } else {
+        const P2 df = psub(b, c);
+        // a - (b + c) / 2 +- i sqrt(3)/2 (b - c): + for k2 = 1 (W_3 = exp(+2 pi i / 3))
+        const P2 y = {f2fma(hf, sm.re, f2fma(make_float2(-s3.x, -s3.y), df.im, a.re)),
+                      f2fma(hf, sm.im, f2fma(s3, df.re, a.im))};
+        v[r] = ptw(y, tw3[(k2 - 1) * M + n1]);
+      }
+    }
+    __syncthreads();  // every thread has read the noise before the transform writes the buffer
+    const P2ArrStore::Tile so = st.tile(p0 + 2 * pq, o, Lout, bad);
+    p2_transform<M, +1>(v, buf, tw, u, q, [&](int k1, const P2& x) {
+      const int j = 3 * k1 + k2;
+      if (j < Lout) st.store_t(so, j, x);
+    });
+    tile = tile_next(ctr, &s_tile, tile, nxt);
+  }
+  p2_report(bad);
+}
+
+// ---------------------------------------------------------------------------
 // Strided complex pass (pencils p, p+1 adjacent), e.g. the middle generation pass.
 // ---------------------------------------------------------------------------
 template <int L, int S>

@@ -501,3 +501,41 @@ def test_cg_fp32_inner_paired_rows(oracle, name):
     assert rep["relative_residual"] <= 1e-8
     assert rel(oracle.matvec(d, lam, pfb200.OP_MUL, x), b) <= 1.1e-8
     P.close()
+
+
+# last-axis lengths 3 M (M = 64 .. 512): the paired noise pass with a radix-3 step
+NOISE3 = {
+    "3d-noise3-192": dict(dim=3, cells=(20, 16, 96), covariance="exponential", corr_length=0.1, approximate=True),
+    "3d-noise3-384": dict(dim=3, cells=(32, 24, 192), covariance="matern32", corr_length=(0.1, 0.2, 0.05),
+                          anisotropy="axiparallel", approximate=True),
+    "2d-noise3-768": dict(dim=2, cells=(40, 384), covariance="gaussian", corr_length=0.05, approximate=True),
+    "2d-noise3-1536": dict(dim=2, cells=(24, 768), covariance="exponential", corr_length=(0.1, 0.05),
+                           anisotropy="axiparallel"),
+    "c5-192cubed": dict(dim=3, cells=(192, 192, 192), covariance="matern32", corr_length=0.1, approximate=True,
+                        transform="logNormal"),
+}
+
+
+@pytest.mark.parametrize("name", list(NOISE3))
+def test_radix3_paired_noise_pass(oracle, name):
+    """FP32 realizations whose noise pass runs the paired kernel with a radix-3 step (last
+    torus axis 3 M), seeded and from a noise buffer, against the FP64 oracle; the c5 case is
+    the 192^3 log-normal workload with its value transform."""
+    cfg = NOISE3[name]
+    d = desc_of(cfg, precision=pfb200.PREC_F32)
+    g = oracle.resolve(d)
+    assert g.T[g.dim - 1] % 3 == 0
+    lam, _, status = oracle.spectrum(d)
+    assert status == 0
+    P = pfb200.Plan(d)
+    P.spectrum_build()
+    tr = "transform" in cfg
+    for seed in (3, 0xABCDEF12345):
+        ref, _ = oracle.generate(d, lam, counter_noise(g, seed, False))
+        if tr:
+            ref = oracle.transform("logNormal", ref)
+        assert rel(P.generate(seed=seed, apply_transform=tr), ref) < TOL32, seed
+    noise = oracle.noise(9, g.noise)
+    ref, _ = oracle.generate(d, lam, noise)
+    assert rel(P.generate(noise=noise), ref) < TOL32
+    P.close()
