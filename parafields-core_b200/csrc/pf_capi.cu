@@ -1208,9 +1208,10 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
     void* src = (char*)W1 + sizeof(cx<T>) * (size_t)w1_plane * z0;
     const double b2 = (double)T0c * nz * (g.T[1] + g.n[1]) * e;
     P->grid_cap = P->tune_grid[1];
-    const bool p2ok = F32 && p2_length(g.T[1]) && p2_view_ok(src, P0, w1_plane, nz) && p2_view_ok(W2, P0, w2_plane, nz);
+    const bool p2ok = F32 && (p2_length(g.T[1]) || p2_length3(g.T[1])) && p2_view_ok(src, P0, w1_plane, nz) &&
+                      p2_view_ok(W2, P0, w2_plane, nz);
     const P2ArrLoad l1 = p2_load(P, src, P0, w1_plane, g.T[1], T0c);
-    if (p2ok && P->tune_variant[1] == 2 && p2_tma_ok(P, l1, nz))  // tiles staged by TMA
+    if (p2ok && P->tune_variant[1] == 2 && p2_length(g.T[1]) && p2_tma_ok(P, l1, nz))  // tiles staged by TMA
       TRY(p2_c2c_tma<+1>(P, "gen_c2c_d1_tma", g.T[1], g.n[1], T0c, nz, l1, p2_store(P, W2, P0, w2_plane, T0c), b2));
     else if (p2ok && P->tune_variant[1] != 1)
       TRY(p2_c2c<+1>(P, "gen_c2c_d1", g.T[1], g.n[1], T0c, nz, l1, p2_store(P, W2, P0, w2_plane, T0c), b2));

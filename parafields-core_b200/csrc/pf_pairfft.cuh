@@ -688,6 +688,39 @@ struct P2Geom3 {
   static_assert(PP * L <= G::Q * G::PLQ, "the tile's noise fits the exchange buffer");
 };
 
+// Radix-3 step and M-point transforms of a tile staged in the exchange buffer (pair g's
+// element n at buf[g L + n]): thread slot q transforms sub-pencil k2 = q % 3 of pair q / 3;
+// Out(j, value) receives output j = 3 k1 + k2.  Sign S of the transform (W = exp(S 2 pi i / .)).
+template <int M, int S, class Out>
+__device__ __forceinline__ void p2_radix3_transform(float4* buf, const float4* tw, const float4* tw3, int u, int q,
+                                                    const Out& out) {
+  using G = P2Geom<M>;
+  constexpr int L = 3 * M;
+  const int pq = q / 3, k2 = q - 3 * (q / 3);
+  const float2 hf = make_float2(-0.5f, -0.5f);
+  // W_3^(k2) = -1/2 + i S sin(2 pi k2 / 3): + sqrt(3)/2 for (S, k2) = (+, 1) and (-, 2)
+  const float sq3 = (k2 == 1) == (S > 0) ? 0.86602540378443865f : -0.86602540378443865f;
+  const float2 s3 = make_float2(sq3, sq3), ns3 = make_float2(-sq3, -sq3);
+  P2 v[8];
+  const float4* xs = buf + pq * L;
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    const int n1 = u + r * G::TP;
+    const P2 a = p2_of(xs[n1]), b = p2_of(xs[n1 + M]), c = p2_of(xs[n1 + 2 * M]);
+    const P2 sm = padd(b, c);
+    if (k2 == 0) {
+      v[r] = padd(a, sm);
+    } else {
+      const P2 df = psub(b, c);
+      // a - (b + c) / 2 + i s3 (b - c)
+      const P2 y = {f2fma(hf, sm.re, f2fma(ns3, df.im, a.re)), f2fma(hf, sm.im, f2fma(s3, df.re, a.im))};
+      v[r] = ptw(y, tw3[(k2 - 1) * M + n1]);
+    }
+  }
+  __syncthreads();  // every thread has read the staged tile before the transform writes the buffer
+  p2_transform<M, S>(v, buf, tw, u, q, [&](int k1, const P2& x) { out(3 * k1 + k2, x); });
+}
+
 template <int M, class Ld>
 __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
     kp2_noise3(const float4* __restrict__ twg, long long ntiles, int tpo, int Lout, Ld ld, P2ArrStore st,
@@ -704,11 +737,8 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
   __syncthreads();
   const int tid = threadIdx.x;
   const int q = tid % G3::QS, u = tid / G3::QS;  // transform: sub-pencil slot, column
-  const int pq = q / 3, k2 = q - 3 * (q / 3);
+  const int pq = q / 3;
   const int gp = tid / (3 * G::TP), gi = tid - gp * (3 * G::TP);  // generation: pair, index
-  const float2 hf = make_float2(-0.5f, -0.5f);
-  const float sq3 = k2 == 1 ? 0.86602540378443865f : -0.86602540378443865f;
-  const float2 s3 = make_float2(sq3, sq3);
   unsigned bad = 0;
   for (long long tile = tile_first(ctr, &s_tile); tile < ntiles;) {
     const unsigned long long nxt = tile_prefetch(ctr);
@@ -739,28 +769,53 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
       }
     }
     __syncthreads();
-    // radix-3 step of sub-pencil k2 and its twiddle W_L^(n1 k2)
-    P2 v[8];
-    const float4* xs = buf + pq * L;
+    const P2ArrStore::Tile so = st.tile(p0 + 2 * pq, o, Lout, bad);
+    p2_radix3_transform<M, +1>(buf, tw, tw3, u, q, [&](int j, const P2& x) {
+      if (j < Lout) st.store_t(so, j, x);
+    });
+    tile = tile_next(ctr, &s_tile, tile, nxt);
+  }
+  p2_report(bad);
+}
+
+// Strided complex pass of length L = 3 M (pencils p, p+1 adjacent): the tile's pencil pairs
+// are staged in the exchange buffer by coalesced pair loads, then the radix-3 step and the
+// paired M-point transforms run as in kp2_noise3.
+template <int M, int S>
+__global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
+    kp2_c2c3(const float4* __restrict__ twg, long long ntiles, int tpo, int Lout, P2ArrLoad ld, P2ArrStore st,
+             unsigned long long* ctr) {
+  __shared__ long long s_tile;
+  using G = P2Geom<M>;
+  using G3 = P2Geom3<M>;
+  constexpr int L = G3::L;
+  extern __shared__ __align__(16) float4 p2_smem[];
+  float4* buf = p2_smem;
+  float4* tw = p2_smem + G::Q * G::PLQ;
+  const float4* tw3 = tw + G::NTW;
+  p2_copy_table(tw, twg, G::NTW + 2 * M);
+  __syncthreads();
+  const int tid = threadIdx.x;
+  const int q = tid % G3::QS, u = tid / G3::QS;
+  const int pq = q / 3;
+  const int gp = tid / (3 * G::TP), gi = tid - gp * (3 * G::TP);
+  unsigned bad = 0;
+  for (long long tile = tile_first(ctr, &s_tile); tile < ntiles;) {
+    const unsigned long long nxt = tile_prefetch(ctr);
+    const int o = (int)(tile / tpo);
+    const int p0 = (int)(tile - (long long)o * tpo) * (2 * G3::PP);
+    {
+      const P2ArrLoad::Tile lt = ld.tile(p0 + 2 * gp, o, bad);
+      float4* xs = buf + gp * L;
 #pragma unroll
-    for (int r = 0; r < 8; r++) {
-      const int n1 = u + r * G::TP;
-      const P2 a = p2_of(xs[n1]), b = p2_of(xs[n1 + M]), c = p2_of(xs[n1 + 2 * M]);
-      const P2 sm = padd(b, c);
-      if (k2 == 0) {
-        v[r] = padd(a, sm);
-      } else {
-        const P2 df = psub(b, c);
-        // a - (b + c) / 2 +- i sqrt(3)/2 (b - c): + for k2 = 1 (W_3 = exp(+2 pi i / 3))
-        const P2 y = {f2fma(hf, sm.re, f2fma(make_float2(-s3.x, -s3.y), df.im, a.re)),
-                      f2fma(hf, sm.im, f2fma(s3, df.re, a.im))};
-        v[r] = ptw(y, tw3[(k2 - 1) * M + n1]);
+      for (int r = 0; r < 8; r++) {
+        const int j = gi + r * (3 * G::TP);
+        xs[j] = slot_of(ld.load_t(lt, j));
       }
     }
-    __syncthreads();  // every thread has read the noise before the transform writes the buffer
+    __syncthreads();
     const P2ArrStore::Tile so = st.tile(p0 + 2 * pq, o, Lout, bad);
-    p2_transform<M, +1>(v, buf, tw, u, q, [&](int k1, const P2& x) {
-      const int j = 3 * k1 + k2;
+    p2_radix3_transform<M, S>(buf, tw, tw3, u, q, [&](int j, const P2& x) {
       if (j < Lout) st.store_t(so, j, x);
     });
     tile = tile_next(ctr, &s_tile, tile, nxt);
