@@ -1168,7 +1168,7 @@ static pf_status gen_r2c(pf_plan* P, const double* noise_dev, uint64_t seed, S* 
     P->grid_cap = P->tune_grid[2];
     const size_t left = (size_t)(g.domain - (size_t)(dst - out));
     if constexpr (F32) {
-      if (P->tune_variant[2] != 1 && g.T[0] % 2 == 0 && p2_length(g.T[0] / 2)) {
+      if (P->tune_variant[2] != 1 && g.T[0] % 2 == 0 && (p2_length(g.T[0] / 2) || p2_length3(g.T[0] / 2))) {
         P2RowLoad rl;
         rl.ptr = (const float2*)src;
         rl.rowstride = (unsigned)P0;

@@ -1186,6 +1186,60 @@ __global__ void __launch_bounds__(kP2Threads, 2)
   p2_report(bad);
 }
 
+// Complex-to-real rows of length L = 3 M (2L reals from L+1 complex, FFTW c2r semantics as
+// kp2_c2r): the rows' pre-processed values Z[m] = (X[m] + conj X[L-m]) + i w^m (X[m] -
+// conj X[L-m]) of the tile's row pairs are staged in the exchange buffer, then the radix-3
+// step and the paired M-point transforms run as in kp2_noise3; output j holds reals 2j, 2j+1.
+template <int M, class St>
+__global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2R)
+    kp2_c2r3(const float4* __restrict__ twg, long long ntiles, int Lout, P2RowLoad ld, St st) {
+  using G = P2Geom<M>;
+  using G3 = P2Geom3<M>;
+  constexpr int L = G3::L;
+  extern __shared__ __align__(16) float4 p2_smem[];
+  float4* buf = p2_smem;
+  float4* tw = p2_smem + G::Q * G::PLQ;
+  const float4* tw3 = tw + G::NTW;          // radix-3 twiddles, 2M entries
+  const float4* twT = tw3 + 2 * M;          // exp(+2 pi i m / 2L), m < L
+  p2_copy_table(tw, twg, G::NTW + 2 * M + L);
+  __syncthreads();
+  const int tid = threadIdx.x;
+  const int q = tid % G3::QS, u = tid / G3::QS;
+  const int pq = q / 3;
+  const int gp = tid / (3 * G::TP), gi = tid - gp * (3 * G::TP);
+  unsigned bad = 0;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int p0 = (int)tile * (2 * G3::PP);
+    {
+      const int p = p0 + 2 * gp;
+      float4* zs = buf + gp * L;
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        const int m = gi + r * (3 * G::TP);
+        float2 xa = ld.one(p, m, bad), xb = ld.one(p + 1, m, bad);
+        float2 ya = ld.one(p, L - m, bad), yb = ld.one(p + 1, L - m, bad);
+        if (m == 0) {
+          xa.y = 0.f;
+          xb.y = 0.f;
+          ya.y = 0.f;
+          yb.y = 0.f;
+        }
+        const P2 X = p2_ab(xa, xb), Y = p2_ab(ya, yb);
+        const P2 sv = {f2add(X.re, Y.re), f2sub(X.im, Y.im)};
+        const P2 dv = {f2sub(X.re, Y.re), f2add(X.im, Y.im)};
+        const P2 t = ptw(dv, twT[m]);
+        zs[m] = slot_of(P2{f2sub(sv.re, t.im), f2add(sv.im, t.re)});
+      }
+    }
+    __syncthreads();
+    const int p = p0 + 2 * pq;
+    p2_radix3_transform<M, +1>(buf, tw, tw3, u, q, [&](int j, const P2& z) {
+      if (2 * j < Lout) st.store(p, j, z, bad);
+    });
+  }
+  p2_report(bad);
+}
+
 // field rows of n0 reals (row p at p * n0) of type O (FP32 fields, or the FP64 vectors of
 // the matvec and the CG), value transform applied in FP32
 template <typename O>

@@ -518,19 +518,25 @@ NOISE3 = {
     "3d-c2c3-768": dict(dim=3, cells=(12, 384, 8), covariance="matern32", corr_length=(0.2, 0.05, 0.2),
                         anisotropy="axiparallel", approximate=True),
     "3d-c2c3-1536": dict(dim=3, cells=(8, 768, 8), covariance="exponential", corr_length=0.05, approximate=True),
+    # complex-to-real rows of length 3 M (T0 / 2 = 384, 768, 1536)
+    "2d-c2r3-384": dict(dim=2, cells=(384, 16), covariance="exponential", corr_length=0.1),
+    "2d-c2r3-768": dict(dim=2, cells=(768, 12), covariance="gaussian", corr_length=0.05, approximate=True),
+    "2d-c2r3-1536": dict(dim=2, cells=(1536, 6), covariance="exponential", corr_length=(0.05, 0.2),
+                         anisotropy="axiparallel"),
 }
 
 
 @pytest.mark.parametrize("name", list(NOISE3))
 def test_radix3_paired_noise_pass(oracle, name):
-    """FP32 realizations whose noise pass (last torus axis 3 M) or strided pass (dim 1 of
-    length 3 M) runs the paired kernels with a radix-3 step, seeded and from a noise buffer,
+    """FP32 realizations whose noise pass (last torus axis 3 M), strided pass (dim 1 of
+    length 3 M) or complex-to-real rows (T0 / 2 = 3 M) run the paired kernels with a radix-3
+    step, seeded and from a noise buffer,
     against the FP64 oracle; the c5 case is the 192^3 log-normal workload with its value
     transform, after measured planning."""
     cfg = NOISE3[name]
     d = desc_of(cfg, precision=pfb200.PREC_F32)
     g = oracle.resolve(d)
-    assert g.T[g.dim - 1] % 3 == 0 or g.T[1] % 3 == 0
+    assert any(g.T[i] % 3 == 0 for i in range(g.dim))
     lam, _, status = oracle.spectrum(d)
     assert status == 0
     P = pfb200.Plan(d)
