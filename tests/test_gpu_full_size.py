@@ -523,6 +523,11 @@ NOISE3 = {
     "2d-c2r3-768": dict(dim=2, cells=(768, 12), covariance="gaussian", corr_length=0.05, approximate=True),
     "2d-c2r3-1536": dict(dim=2, cells=(1536, 6), covariance="exponential", corr_length=(0.05, 0.2),
                          anisotropy="axiparallel"),
+    # the other eigenvalue layouts and the untransposed 3D order under the radix-3 noise pass
+    "3d-noise3-r2c-untransposed": dict(dim=3, cells=(24, 16, 96), covariance="exponential", corr_length=0.1,
+                                       approximate=True, matrix_backend=pfb200.MATRIX_R2C, transposed=0),
+    "2d-noise3-dftmatrix": dict(dim=2, cells=(20, 192), covariance="matern32", corr_length=0.1, approximate=True,
+                                matrix_backend=pfb200.MATRIX_DFT),
 }
 
 
