@@ -691,31 +691,34 @@ struct P2Geom3 {
 // Radix-3 step and M-point transforms of a tile staged in the exchange buffer (pair g's
 // element n at buf[g L + n]): thread slot q transforms sub-pencil k2 = q % 3 of pair q / 3;
 // Out(j, value) receives output j = 3 k1 + k2.  Sign S of the transform (W = exp(S 2 pi i / .)).
+// output k2 of the radix-3 butterfly of (a, b, c) (elements n1, n1 + M, n1 + 2M), times the
+// twiddle w = W_L^(n1 k2) (unused for k2 = 0)
+template <int S>
+__device__ __forceinline__ P2 p2_radix3_point(const P2& a, const P2& b, const P2& c, int k2, float4 w) {
+  const P2 sm = padd(b, c);
+  if (k2 == 0) return padd(a, sm);
+  // W_3^(k2) = -1/2 + i S sin(2 pi k2 / 3): + sqrt(3)/2 for (S, k2) = (+, 1) and (-, 2)
+  const float sq3 = (k2 == 1) == (S > 0) ? 0.86602540378443865f : -0.86602540378443865f;
+  const float2 hf = make_float2(-0.5f, -0.5f), s3 = make_float2(sq3, sq3), ns3 = make_float2(-sq3, -sq3);
+  const P2 df = psub(b, c);
+  // a - (b + c) / 2 + i s3 (b - c)
+  const P2 y = {f2fma(hf, sm.re, f2fma(ns3, df.im, a.re)), f2fma(hf, sm.im, f2fma(s3, df.re, a.im))};
+  return ptw(y, w);
+}
+
 template <int M, int S, class Out>
 __device__ __forceinline__ void p2_radix3_transform(float4* buf, const float4* tw, const float4* tw3, int u, int q,
                                                     const Out& out) {
   using G = P2Geom<M>;
   constexpr int L = 3 * M;
   const int pq = q / 3, k2 = q - 3 * (q / 3);
-  const float2 hf = make_float2(-0.5f, -0.5f);
-  // W_3^(k2) = -1/2 + i S sin(2 pi k2 / 3): + sqrt(3)/2 for (S, k2) = (+, 1) and (-, 2)
-  const float sq3 = (k2 == 1) == (S > 0) ? 0.86602540378443865f : -0.86602540378443865f;
-  const float2 s3 = make_float2(sq3, sq3), ns3 = make_float2(-sq3, -sq3);
   P2 v[8];
   const float4* xs = buf + pq * L;
 #pragma unroll
   for (int r = 0; r < 8; r++) {
     const int n1 = u + r * G::TP;
-    const P2 a = p2_of(xs[n1]), b = p2_of(xs[n1 + M]), c = p2_of(xs[n1 + 2 * M]);
-    const P2 sm = padd(b, c);
-    if (k2 == 0) {
-      v[r] = padd(a, sm);
-    } else {
-      const P2 df = psub(b, c);
-      // a - (b + c) / 2 + i s3 (b - c)
-      const P2 y = {f2fma(hf, sm.re, f2fma(ns3, df.im, a.re)), f2fma(hf, sm.im, f2fma(s3, df.re, a.im))};
-      v[r] = ptw(y, tw3[(k2 - 1) * M + n1]);
-    }
+    v[r] = p2_radix3_point<S>(p2_of(xs[n1]), p2_of(xs[n1 + M]), p2_of(xs[n1 + 2 * M]), k2,
+                              k2 ? tw3[(k2 - 1) * M + n1] : make_float4(1.f, 1.f, 0.f, 0.f));
   }
   __syncthreads();  // every thread has read the staged tile before the transform writes the buffer
   p2_transform<M, S>(v, buf, tw, u, q, [&](int k1, const P2& x) { out(3 * k1 + k2, x); });
@@ -778,9 +781,9 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_NOISE)
   p2_report(bad);
 }
 
-// Strided complex pass of length L = 3 M (pencils p, p+1 adjacent): the tile's pencil pairs
-// are staged in the exchange buffer by coalesced pair loads, then the radix-3 step and the
-// paired M-point transforms run as in kp2_noise3.
+// Strided complex pass of length L = 3 M (pencils p, p+1 adjacent): every thread loads the
+// three inputs of its radix-3 butterflies itself, then the paired M-point transforms run as
+// in kp2_noise3.
 template <int M, int S>
 __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
     kp2_c2c3(const float4* __restrict__ twg, long long ntiles, int tpo, int Lout, P2ArrLoad ld, P2ArrStore st,
@@ -788,7 +791,6 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
   __shared__ long long s_tile;
   using G = P2Geom<M>;
   using G3 = P2Geom3<M>;
-  constexpr int L = G3::L;
   extern __shared__ __align__(16) float4 p2_smem[];
   float4* buf = p2_smem;
   float4* tw = p2_smem + G::Q * G::PLQ;
@@ -797,25 +799,25 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2C)
   __syncthreads();
   const int tid = threadIdx.x;
   const int q = tid % G3::QS, u = tid / G3::QS;
-  const int pq = q / 3;
-  const int gp = tid / (3 * G::TP), gi = tid - gp * (3 * G::TP);
+  const int pq = q / 3, k2 = q - 3 * (q / 3);
   unsigned bad = 0;
   for (long long tile = tile_first(ctr, &s_tile); tile < ntiles;) {
     const unsigned long long nxt = tile_prefetch(ctr);
     const int o = (int)(tile / tpo);
     const int p0 = (int)(tile - (long long)o * tpo) * (2 * G3::PP);
-    {
-      const P2ArrLoad::Tile lt = ld.tile(p0 + 2 * gp, o, bad);
-      float4* xs = buf + gp * L;
+    // the three inputs of each radix-3 butterfly straight from global memory (the three
+    // threads of a pencil pair that share them read the same addresses, served by L1)
+    const P2ArrLoad::Tile lt = ld.tile(p0 + 2 * pq, o, bad);
+    P2 v[8];
 #pragma unroll
-      for (int r = 0; r < 8; r++) {
-        const int j = gi + r * (3 * G::TP);
-        xs[j] = slot_of(ld.load_t(lt, j));
-      }
+    for (int r = 0; r < 8; r++) {
+      const int n1 = u + r * G::TP;
+      v[r] = p2_radix3_point<S>(ld.load_t(lt, n1), ld.load_t(lt, n1 + M), ld.load_t(lt, n1 + 2 * M), k2,
+                                k2 ? tw3[(k2 - 1) * M + n1] : make_float4(1.f, 1.f, 0.f, 0.f));
     }
-    __syncthreads();
     const P2ArrStore::Tile so = st.tile(p0 + 2 * pq, o, Lout, bad);
-    p2_radix3_transform<M, S>(buf, tw, tw3, u, q, [&](int j, const P2& x) {
+    p2_transform<M, S>(v, buf, tw, u, q, [&](int k1, const P2& x) {
+      const int j = 3 * k1 + k2;
       if (j < Lout) st.store_t(so, j, x);
     });
     tile = tile_next(ctr, &s_tile, tile, nxt);
