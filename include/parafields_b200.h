@@ -414,9 +414,10 @@ pf_status pf_plan_set_preconditioner(pf_plan* plan, pf_learned* learned);
 /* Measured planning, the counterpart of fftw.measure / fftw.useWisdom (r2cfieldbackend.hh:
  * 212-230, fieldtraits.hh:175-186): times every candidate of each realization pass of the
  * plan (paired-FP32 or scalar kernels x resident CTAs per SM of the persistent kernels,
- * `repetitions` realizations each, default 3) and keeps the fastest per pass; then, on
- * batches of 4 realizations, the plane groups of the last two 3D passes and the batch mode
- * of pf_generate_batch.  Choices go to
+ * `repetitions` realizations each, default 3) and keeps the fastest per pass (a pass whose
+ * paired and scalar kernels come within 10% is decided on a batch); then, on batches of 4
+ * realizations, the plane groups of the last two 3D passes and the batch mode of
+ * pf_generate_batch.  Choices go to
  * a process-wide wisdom table keyed by the pass geometry; a plan whose passes are all in it
  * takes them without timing (*timed = 0).  Clears the plan's profiling records.  R2C field
  * backend only (other plans: no-op). */
