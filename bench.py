@@ -286,6 +286,14 @@ def run_b200(args):
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     launches = P.launch_count() - l0
+    # the drop-in use, one pf_generate call per realization (as RandomField::generate drives the
+    # matrix), device output: reported beside the line, not the headline
+    e0.record(stream)
+    for i in range(args.steps):
+        P.generate(seed=seed0 + 200 + i, out=out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_one = max_over_ranks(e0.elapsed_time(e1), world, dev)
     # per-kernel durations for the roofline: the same realizations one at a time (no overlap)
     P.profile(True)
     for i in range(args.steps):
@@ -403,6 +411,11 @@ def run_b200(args):
                                 "every realization copied to the host inside the region while the next one is "
                                 "computed (wall clock)"},
                 "rel_l2_error_vs_oracle": err["rel_l2_error_vs_oracle"] if err else None, "error": err,
+                "one_at_a_time": {"value": aggregate_rate(world, n, args.steps, ms_one / 1e3), "unit": "cells/s",
+                                  "ms_per_step": ms_one / args.steps,
+                                  "note": "pf_generate per realization (device output), no overlap between "
+                                          "realizations"},
+                "planning": pfb200.wisdom_export().strip().splitlines(),
                 "gpu_launches": launches, "roofline": roof, "compute": compute, "cpu_baseline": cpu,
                 "cpu_baseline_library_fft": cpu_lib,
                 "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"],
