@@ -13,6 +13,7 @@ namespace pf {
 struct CgScratch {
   double *Ax = nullptr, *r = nullptr, *z = nullptr, *d = nullptr, *Ad = nullptr, *e = nullptr, *ri = nullptr;
   double *part = nullptr, *s = nullptr;
+  unsigned* cnt = nullptr;  // ticket of the last-block reductions (0 between kernels)
   double* hs = nullptr;  // pinned copy of the scalars
   uint64_t n = 0;
 };
@@ -53,15 +54,47 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return r;
 }
 
-// out[blk] = sum a_i * b_i
-__global__ void __launch_bounds__(kCgThreads) k_dot(const double* __restrict__ a, const double* __restrict__ b,
-                                                    uint64_t n, double* part) {
+// Reductions finished inside the kernel: every block stores its partial, and the last block
+// to take a ticket on `cnt` (which it resets to 0 for the next kernel of the stream) sums the
+// partials in the fixed order of k_finish below, so the result is the same, bit for bit, as
+// with the separate finishing kernel.
+__device__ __forceinline__ bool cg_last_block(double v, double* part, unsigned* cnt) {
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = v;
+    __threadfence();  // the partial is visible before the ticket is taken
+    last = atomicAdd(cnt, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  return last;
+}
+__device__ __forceinline__ double cg_sum_partials(const double* part, double* sh) {
+  __threadfence();
+  double v = 0.;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) v += __ldcg(part + i);
+  return block_sum(v, sh);
+}
+
+// s[slot] = sum a_i * b_i; with beta set, then beta = SPNEW / SP and SP <- SPNEW
+// (matrix.hh:1409-1417), nothing of which once a residual-mode inner solve stopped
+__global__ void __launch_bounds__(kCgThreads) k_dot_fin(const double* __restrict__ a, const double* __restrict__ b,
+                                                        uint64_t n, double* part, unsigned* cnt, double* s, int slot,
+                                                        int beta) {
   __shared__ double sh[32];
-  double s = 0.;
+  double v = 0.;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-    s += a[i] * b[i];
-  s = block_sum(s, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = s;
+    v += a[i] * b[i];
+  v = block_sum(v, sh);
+  if (!cg_last_block(v, part, cnt)) return;
+  const double t = cg_sum_partials(part, sh);
+  if (threadIdx.x == 0) {
+    s[slot] = t;
+    if (beta && s[S_DONE] == 0.) {
+      s[S_BETA] = s[S_SPNEW] / s[S_SP];
+      s[S_SP] = s[S_SPNEW];
+    }
+    *cnt = 0u;
+  }
 }
 
 // part[2 blk] = d . Ad, part[2 blk + 1] = x . (0.5 Ax - b)  (matrix.hh:1373-1386)
@@ -115,14 +148,6 @@ __global__ void k_finish(const double* part, int nblk, int nout, double* s, int 
   }
 }
 
-// beta = SPNEW / SP (matrix.hh:1409-1417); SP <- SPNEW.  Nothing once the inner solve
-// stopped (S_DONE is never set in reference mode).
-__global__ void k_cg_beta(double* s) {
-  if (s[S_DONE] != 0.) return;
-  s[S_BETA] = s[S_SPNEW] / s[S_SP];
-  s[S_SP] = s[S_SPNEW];
-}
-
 // d = z + beta d
 __global__ void __launch_bounds__(kCgThreads) k_cg_dir(double* __restrict__ d, const double* __restrict__ z, uint64_t n,
                                                        const double* s) {
@@ -138,14 +163,17 @@ __global__ void k_sub(const double* __restrict__ b, const double* __restrict__ A
     r[i] = b[i] - Ax[i];
 }
 
-// residual-mode PCG update: x += alpha d, r -= alpha Ad (alpha = SP / DEN); part = r . r.
-// Nothing once the inner solve stopped: the host checks S_DONE only every few
-// iterations, and the iterations launched after the stop leave x and r unchanged.
-__global__ void __launch_bounds__(kCgThreads) k_pcg_update(double* __restrict__ x, double* __restrict__ r,
-                                                           const double* __restrict__ d, const double* __restrict__ Ad,
-                                                           uint64_t n, const double* s, double* part) {
+// residual-mode PCG update: x += alpha d, r -= alpha Ad (alpha = SP / DEN), r . r into S_RR,
+// then the stopping test by the last block: count the iteration, stop on r . r <= S_THR
+// (S_DONE = 1) or a NaN residual (S_DONE = 2).  Nothing once the inner solve stopped: the
+// host reads S_DONE only every few iterations, and the iterations launched after the stop
+// leave x and r unchanged.
+__global__ void __launch_bounds__(kCgThreads) k_pcg_update_fin(double* __restrict__ x, double* __restrict__ r,
+                                                               const double* __restrict__ d,
+                                                               const double* __restrict__ Ad, uint64_t n, double* s,
+                                                               double* part, unsigned* cnt) {
   __shared__ double sh[32];
-  if (s[S_DONE] != 0.) return;
+  if (s[S_DONE] != 0.) return;  // every block: no partial, no ticket
   const double alpha = s[S_SP] / s[S_DEN];
   double v = 0.;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -155,7 +183,17 @@ __global__ void __launch_bounds__(kCgThreads) k_pcg_update(double* __restrict__ 
     v += ri * ri;
   }
   v = block_sum(v, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = v;
+  if (!cg_last_block(v, part, cnt)) return;
+  const double rr = cg_sum_partials(part, sh);
+  if (threadIdx.x == 0) {
+    s[S_RR] = rr;
+    s[S_ITERS] += 1.;
+    if (!(rr == rr))
+      s[S_DONE] = 2.;
+    else if (rr <= s[S_THR])
+      s[S_DONE] = 1.;
+    *cnt = 0u;
+  }
 }
 
 // start of a residual-mode inner solve: stop threshold on r . r, counters cleared
@@ -163,17 +201,6 @@ __global__ void k_pcg_start(double* s, double thr) {
   s[S_DONE] = 0.;
   s[S_ITERS] = 0.;
   s[S_THR] = thr;
-}
-
-// after an update: count the iteration, stop on convergence or a NaN residual
-__global__ void k_pcg_check(double* s) {
-  if (s[S_DONE] != 0.) return;
-  s[S_ITERS] += 1.;
-  const double rr = s[S_RR];
-  if (!(rr == rr))
-    s[S_DONE] = 2.;
-  else if (rr <= s[S_THR])
-    s[S_DONE] = 1.;
 }
 
 __global__ void k_axpy(double* __restrict__ y, const double* __restrict__ x, uint64_t n) {
