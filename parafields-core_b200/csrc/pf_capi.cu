@@ -267,6 +267,10 @@ struct pf_plan {
   // kernels that run at the same time never share a counter
   unsigned long long* tile_ctr = nullptr;
   int ctr_slot = 0;
+  // residual-mode CG: the next matvec's input d is first updated to z + beta d inside its
+  // first pass (set around one matvec call by the CG driver; cg_dir_fusable says when)
+  const double* cg_dir_z = nullptr;
+  const double* cg_dir_s = nullptr;
 };
 
 static pf_status dalloc(pf_plan* P, void** p, size_t bytes) {
@@ -1364,6 +1368,19 @@ static pf_status matvec_r2c(pf_plan* P, int op, const S* in, S* out) {
   const int pair_ok = (g.n[0] % 2 == 0) ? 1 : 0;
   auto fwd_rows = [&](void* X, long long nrows) -> pf_status {
     const double b = (double)nrows * (g.n[0] * sizeof(S) + T0c * e);
+    if (P->cg_dir_z) {  // CG direction update fused into this pass (FP32 transforms, FP64 vectors)
+      if constexpr (std::is_same<T, float>::value && std::is_same<S, double>::value) {
+        if (p2rows) {
+          const bool al = ((uintptr_t)in % 16) == 0 && ((uintptr_t)P->cg_dir_z % 16) == 0;
+          P2DirRowLoad dl{P->cg_dir_z, const_cast<double*>(in), P->cg_dir_s, g.n[0], (unsigned)g.domain,
+                          (int)nrows, pair_ok && al ? 1 : 0};
+          P2RowStore rs{(float2*)X, (unsigned)P0, (unsigned)std::min<size_t>(cap_of(P, X) / sizeof(float2), 0xffffffffu),
+                        (int)nrows, T0c};
+          return p2_r2c(P, "mv_r2c_d0", g.T[0] / 2, nrows, dl, rs, b + (double)nrows * g.n[0] * 16.0);
+        }
+      }
+      return fail(PF_ERR_STATE, "internal error: fused direction update on a matvec without paired rows");
+    }
     if constexpr (std::is_same<T, float>::value) {
       if (p2rows) {
         P2RealRowLoad<S> rl{in, g.n[0], (unsigned)g.domain, (int)nrows,
@@ -1506,6 +1523,13 @@ static pf_status matvec_dev(pf_plan* P, int op, const S* in, S* out) {
 // internal operation: torus pseudo-inverse (clamped eigenvalues dropped), used as the
 // preconditioner of the residual-mode CG
 constexpr int kOpInvPinv = 3;
+
+// whether the FP32 matvec of plan P takes the paired real-to-complex rows, into which the
+// residual-mode CG folds its direction update (P2DirRowLoad)
+static bool cg_dir_fusable(const pf_plan* P, bool fp32) {
+  const Geom& g = P->g;
+  return fp32 && (g.fb == PF_FIELD_R2C || g.fb == PF_FIELD_DCTDST) && g.T[0] % 2 == 0 && p2_length(g.T[0] / 2);
+}
 
 // CG helpers use FP64 vectors with FP64 or FP32 transforms
 static pf_status cg_matvec(pf_plan* P, int op, bool fp32, const double* in, double* out) {

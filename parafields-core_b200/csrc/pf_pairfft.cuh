@@ -19,6 +19,7 @@
 
 #include <cuda.h>
 
+#include "pf_cg.cuh"
 #include "pf_fastfft.cuh"
 
 namespace pf {
@@ -1317,6 +1318,50 @@ struct P2RealRowLoad {
     z.x = (float)x[i];
     if (two) z.y = (float)x[i + 1];
     return z;
+  }
+};
+
+// FP64 rows of the CG's search direction, updated on the way into the matvec: d = z + beta d
+// (beta = s[S_BETA]; no update once a residual-mode inner solve stopped, s[S_DONE] != 0),
+// written back to d and returned in FP32 as P2RealRowLoad does.  Each element is loaded by
+// exactly one thread of kp2_r2c, so the write-back has one writer.
+struct P2DirRowLoad {
+  const double* z;
+  double* d;
+  const double* s;
+  int n0;
+  unsigned n;
+  int np;
+  int vec;  // z and d 16-byte aligned and n0 even
+  __device__ __forceinline__ float2 pair(int p, int m, unsigned& bad) const {
+    float2 out = make_float2(0.f, 0.f);
+    if (p >= np || 2 * m >= n0) return out;
+    const unsigned i = (unsigned)p * (unsigned)n0 + 2u * (unsigned)m;
+    const bool two = 2 * m + 1 < n0;
+    const bool ok = i + (two ? 1u : 0u) < n;
+    bad |= (unsigned)!ok;
+    if (!ok) return out;
+    const bool upd = s[S_DONE] == 0.;
+    const double beta = s[S_BETA];
+    if (two && vec) {
+      const double2 zz = *reinterpret_cast<const double2*>(z + i);
+      double2 dd = *reinterpret_cast<const double2*>(d + i);
+      if (upd) {
+        dd.x = zz.x + beta * dd.x;
+        dd.y = zz.y + beta * dd.y;
+        *reinterpret_cast<double2*>(d + i) = dd;
+      }
+      return make_float2((float)dd.x, (float)dd.y);
+    }
+    double a = d[i];
+    if (upd) d[i] = a = z[i] + beta * a;
+    out.x = (float)a;
+    if (two) {
+      double b = d[i + 1];
+      if (upd) d[i + 1] = b = z[i + 1] + beta * b;
+      out.y = (float)b;
+    }
+    return out;
   }
 };
 
