@@ -271,6 +271,9 @@ struct pf_plan {
   // first pass (set around one matvec call by the CG driver; cg_dir_fusable says when)
   const double* cg_dir_z = nullptr;
   const double* cg_dir_s = nullptr;
+  // residual-mode CG: the same matvec's last pass also sums cg_dot_d . out into *cg_dot_dst
+  const double* cg_dot_d = nullptr;
+  double* cg_dot_dst = nullptr;
 };
 
 static pf_status dalloc(pf_plan* P, void** p, size_t bytes) {
@@ -1394,6 +1397,33 @@ static pf_status matvec_r2c(pf_plan* P, int op, const S* in, S* out) {
   };
   auto inv_rows = [&](void* X, long long nrows) -> pf_status {
     const double b = (double)nrows * (T0c * e + g.n[0] * sizeof(S));
+    if (P->cg_dot_d) {  // CG: d . (A d) summed in this pass (FP32 transforms, FP64 vectors)
+      if constexpr (std::is_same<T, float>::value && std::is_same<S, double>::value) {
+        if (p2rows) {
+          P2RowLoad rl;
+          rl.ptr = (const float2*)X;
+          rl.rowstride = (unsigned)P0;
+          rl.n = (unsigned)std::min<size_t>(cap_of(P, X) / sizeof(float2), 0xffffffffu);
+          rl.Lin = T0c;
+          rl.np = (int)nrows;
+          P2FieldDotStore ps;
+          ps.out = out;
+          ps.n0 = g.n[0];
+          ps.transform = 0;
+          ps.boxcox = 0.f;
+          ps.n = (unsigned)g.domain;
+          ps.np = (int)nrows;
+          ps.Lout = g.n[0];
+          ps.vec = pair_ok && ((uintptr_t)out % 16) == 0 ? 1 : 0;
+          ps.dv = P->cg_dot_d;
+          ps.part = P->cg.part;  // 2 kCgBlocks doubles: more than any persistent grid's CTAs
+          ps.cnt = P->cg.cnt;
+          ps.sdst = P->cg_dot_dst;
+          return p2_c2r(P, "mv_c2r_d0", g.T[0] / 2, g.n[0], nrows, rl, ps, b + (double)nrows * g.n[0] * 8.0);
+        }
+      }
+      return fail(PF_ERR_STATE, "internal error: fused dot product on a matvec without paired rows");
+    }
     if constexpr (std::is_same<T, float>::value) {
       if (p2rows) {
         P2RowLoad rl;

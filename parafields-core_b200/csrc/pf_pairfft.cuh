@@ -1049,6 +1049,7 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2R)
   __syncthreads();
   const int u = threadIdx.x % G::TP, q = threadIdx.x / G::TP;
   unsigned bad = 0;
+  [[maybe_unused]] double acc = 0.;  // St::kDot: this thread's share of the dot product
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int p = (int)tile * G::NP + 2 * q;
     P2 v[8];
@@ -1071,8 +1072,22 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2R)
       v[r] = {f2sub(s.re, t.im), f2add(s.im, t.re)};
     }
     p2_transform<L, +1>(v, buf, tw, u, q, [&](int m, const P2& z) {
-      if (2 * m < Lout) st.store(p, m, z, bad);
+      if (2 * m < Lout) {
+        st.store(p, m, z, bad);
+        if constexpr (St::kDot) acc += st.dot(p, m, z);
+      }
     });
+  }
+  if constexpr (St::kDot) {  // a . out over the stored values, finished by the last block
+    __shared__ double shd[32];
+    acc = block_sum(acc, shd);
+    if (cg_last_block(acc, st.part, st.cnt)) {
+      const double t = cg_sum_partials(st.part, shd);
+      if (threadIdx.x == 0) {
+        *st.sdst = t;
+        *st.cnt = 0u;
+      }
+    }
   }
   p2_report(bad);
 }
@@ -1248,6 +1263,7 @@ __global__ void __launch_bounds__(kP2Threads, PF_P2_MIN_C2R)
 template <typename O>
 struct P2FieldStoreT {
   using O2 = typename std::conditional<sizeof(O) == 8, double2, float2>::type;
+  static constexpr bool kDot = false;
   O* out;
   int n0;
   int transform;
@@ -1283,6 +1299,30 @@ struct P2FieldStoreT {
   }
 };
 using P2FieldStore = P2FieldStoreT<float>;
+
+// FP64 rows of the matvec's output that also accumulate dv . out over the stored values
+// (the CG's d . A d); kp2_c2r finishes the sum with the last-block reduction into *sdst.
+// Every output element is stored exactly once, so every product enters once; the order of
+// the sum is fixed by the kernel's static tile order.
+struct P2FieldDotStore : P2FieldStoreT<double> {
+  static constexpr bool kDot = true;
+  const double* dv;
+  double* part;   // one partial per CTA
+  unsigned* cnt;  // ticket, 0 between kernels
+  double* sdst;
+  __device__ __forceinline__ double dot1(int p, int m, float a, float b) const {
+    if (p >= np) return 0.;
+    const unsigned i = (unsigned)p * (unsigned)n0 + 2u * (unsigned)m;
+    const bool two = 2 * m + 1 < Lout;
+    if (i + (two ? 1u : 0u) >= n) return 0.;
+    double r = dv[i] * (double)a;
+    if (two) r += dv[i + 1] * (double)b;
+    return r;
+  }
+  __device__ __forceinline__ double dot(int p, int m, const P2& z) const {
+    return dot1(p, m, z.re.x, z.im.x) + dot1(p + 1, m, z.re.y, z.im.y);
+  }
+};
 
 // ---------------------------------------------------------------------------
 // Real-to-complex rows (L+1 complex from 2L reals, FFTW r2c semantics), the forward
